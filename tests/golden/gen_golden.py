@@ -1,0 +1,111 @@
+"""Generates the golden fixtures in this directory from the reference's own
+code (oracle/_ref, built from the reference sources by oracle/build_ref.sh).
+
+Run from the repository root in a container that has the reference tree:
+    python tests/golden/gen_golden.py
+
+Fixtures:
+  intersect_simple.npz     reference test Intersect_Simple
+                           (src/lightmetrica.test/test.scene.intersection.cpp:117-151)
+  intersect_simple2.npz    reference test Intersect_Simple2 (:153-187)
+  consistency_random.npz   reference test Consistency (:190-266) on
+                           StubTriangleMesh_Random (stub.trianglemesh.h:184-225)
+  soup_small.npz           seeded triangle soup with the ray-intersection
+                           benchmark's distributions (4096 tris, edge sigma
+                           0.16, 8192 rays);
+                           reference BVHScene tri ids, t and (u, v)
+Each fixture stores the inputs with the reference outputs for every scene
+type the reference builds here (bvh, qbvh, naive).
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from lightmetrica_b200.workloads import random_rays, random_soup, FLT_MAX  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+TYPES = ("bvh", "qbvh", "naive")
+
+
+def _grid_rays(origin_fn, dir_fn):
+    rays = []
+    for i in range(1, 10):
+        y = np.float32(0.1) * np.float32(i)
+        for j in range(1, 10):
+            x = np.float32(0.1) * np.float32(j)
+            o = origin_fn(x, y)
+            d = dir_fn(x, y, o)
+            rays.append([*o, *d, 0.0, FLT_MAX])
+    return np.asarray(rays, np.float32)
+
+
+def _run_all(name, pos, faces, normals, texcoords, rays, extra=None):
+    out = dict(positions=pos, faces=faces, rays=rays)
+    if normals is not None:
+        out["normals"] = normals
+    if texcoords is not None:
+        out["texcoords"] = texcoords
+    for typ in TYPES:
+        s = oracle.RefScene(pos, faces, typ, normals=normals, texcoords=texcoords)
+        r = s.intersect(rays, geom=True)
+        for k in ("tri_id", "t", "p", "gn", "sn", "ss", "st", "uv"):
+            out[f"{typ}_{k}"] = r[k]
+    if extra:
+        out.update(extra)
+    np.savez_compressed(os.path.join(OUT, name), **out)
+    print("wrote", name, {k: v.shape for k, v in out.items()})
+
+
+def main():
+    if not oracle.ref_available("f"):
+        raise SystemExit("oracle/_ref/liblmref_f.so missing: run oracle/build_ref.sh first")
+
+    # Intersect_Simple: two z-planes, rays from (0,0,1) towards (x,y,0)
+    ps = np.array([0, 0, 0, 1, 0, 0, 1, 1, 0, 0, 1, 0, 0, 0, -1, 1, 0, -1, 1, 1, -1, 0, 1, -1], np.float32).reshape(-1, 3)
+    ns = np.tile(np.array([0, 0, 1], np.float32), (8, 1))
+    ts = np.array([0, 0, 1, 0, 1, 1, 0, 1] * 2, np.float32).reshape(-1, 2)
+    fs = np.array([0, 1, 2, 0, 2, 3, 4, 5, 6, 4, 6, 7], np.uint32).reshape(-1, 3)
+
+    def d_simple(x, y, o):
+        d = np.array([x, y, 0], np.float64) - np.asarray(o, np.float64)
+        return (d / np.linalg.norm(d)).astype(np.float32)
+    rays = _grid_rays(lambda x, y: np.array([0, 0, 1], np.float32), d_simple)
+    _run_all("intersect_simple.npz", ps, fs, ns, ts, rays)
+
+    # Intersect_Simple2: slanted plane x = -z, vertical rays
+    ps2 = np.array([0, 0, 0, 1, 0, -1, 1, 1, -1, 0, 1, 0], np.float32).reshape(-1, 3)
+    n2 = (np.array([1, 0, 1], np.float64) / np.sqrt(2.0)).astype(np.float32)
+    ns2 = np.tile(n2, (4, 1))
+    ts2 = np.array([0, 0, 1, 0, 1, 1, 0, 1], np.float32).reshape(-1, 2)
+    fs2 = np.array([0, 1, 2, 0, 2, 3], np.uint32).reshape(-1, 3)
+    rays2 = _grid_rays(lambda x, y: np.array([x, y, 1], np.float32), lambda x, y, o: np.array([0, 0, -1], np.float32))
+    _run_all("intersect_simple2.npz", ps2, fs2, ns2, ts2, rays2)
+
+    # Consistency: 1000 random triangles in [0,1]^3, vertical rays
+    pr, nr = oracle.stub_random_mesh()
+    fr = np.arange(3000, dtype=np.uint32).reshape(-1, 3)
+    rays3 = _grid_rays(lambda x, y: np.array([x, y, 1], np.float32), lambda x, y, o: np.array([0, 0, -1], np.float32))
+    _run_all("consistency_random.npz", pr, fr, nr, None, rays3)
+
+    # Benchmark-distribution soup, small: ids, t and barycentrics (uv = b
+    # because the harness assigns corner texcoords (0,0),(1,0),(0,1)). Edge
+    # sigma is scaled by sqrt(1M / 4096) = 16 so that the hit rate matches the
+    # 1M-triangle benchmark scene's (about a quarter of the rays).
+    pos, faces = random_soup(4096, seed=11, sigma=0.16)
+    rays4 = random_rays(8192, seed=12)
+    s = oracle.RefScene(pos, faces, "bvh")
+    r = s.intersect(rays4, geom=True)
+    np.savez_compressed(os.path.join(OUT, "soup_small.npz"), positions=pos, faces=faces, rays=rays4,
+                        bvh_tri_id=r["tri_id"], bvh_t=r["t"], bvh_u=r["uv"][:, 0], bvh_v=r["uv"][:, 1])
+    print("wrote soup_small.npz hits", int((r["tri_id"] >= 0).sum()))
+
+
+if __name__ == "__main__":
+    main()
