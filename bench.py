@@ -1,0 +1,377 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 scene accelerator / path tracer.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload intersect|render]
+
+Prints ONE JSON line on rank 0. Multi-GPU runs (torchrun, one process per
+GPU) are independent replicas with weak scaling: every rank traces its own
+seeded ray batch against its own copy of the scene; there is no data-path
+collective. The job time is the max over ranks of the device time.
+
+Workload `intersect` (the default): 2^24 rays (origins U[-2,2]^3, directions
+uniform on the sphere) against 1,048,576 random triangles (centres U[-1,1]^3,
+edges N(0, 0.01^2)), closest hit with the binary SAH BVH that reproduces the
+reference BVHScene. One step = one launch over the whole ray batch, which is
+larger than L2 (512 MB of rays), so no L2 flush is needed between steps.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NUM_TRIS = 1 << 20
+NUM_RAYS = 1 << 24
+NODE_BYTES = 32      # compact binary node (6 f32 + 2 u32), per slab test
+TRI_BYTES = 48       # TriAccel record, per triangle test
+RAY_IO_BYTES = 32 + 16
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="intersect", choices=["intersect"])
+    ap.add_argument("--layout", default="bvh", choices=["bvh", "qbvh"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_traffic(layout):
+    """Per-launch DRAM bytes of the traversal kernel from the committed ncu
+    summary (profiles/), or None."""
+    p = os.path.join(ROOT, "profiles", f"trace_closest_{layout}_intersect.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f).get("dram_bytes_per_launch_full")
+    return None
+
+
+# --------------------------------------------------------------- reference --
+
+def cpu_reference_rate(pos, faces, rays, budget_s=12.0, threads=None):
+    """The reference's own BVHScene (oracle/_ref, compiled from the reference
+    sources) on the host cores: Mrays/s over a bounded sample of `rays`."""
+    import oracle
+    threads = threads or os.cpu_count() or 1
+    if oracle.ref_available("f"):
+        sc = oracle.RefScene(pos, faces, "bvh")
+        kind = "reference"
+        trace = lambda r: sc.intersect(r, threads=threads)  # noqa: E731
+    else:
+        sc = oracle.OracleScene(pos, faces, "bvh")
+        kind = "port"
+        threads = 1
+        trace = lambda r: sc.intersect(r)  # noqa: E731
+    n, done, t_total = 1 << 16, 0, 0.0
+    while t_total < budget_s and done < rays.shape[0]:
+        m = min(n, rays.shape[0] - done)
+        t0 = time.perf_counter()
+        trace(rays[done:done + m])
+        t_total += time.perf_counter() - t0
+        done += m
+        n = min(n * 2, 1 << 22)
+    return done / t_total / 1e6, kind, threads, done, t_total
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from lightmetrica_b200.workloads import random_rays, random_soup
+    pos, faces = random_soup(NUM_TRIS, seed=1)
+    rays = random_rays(1 << 22, seed=2)
+    import oracle
+    threads = os.cpu_count() or 1
+    if oracle.ref_available("f"):
+        sc = oracle.RefScene(pos, faces, "bvh")
+        kind = "reference"
+        trace = lambda r: sc.intersect(r, threads=threads)  # noqa: E731
+    else:
+        sc = oracle.OracleScene(pos, faces, "bvh")
+        kind, threads = "port", 1
+        trace = lambda r: sc.intersect(r)  # noqa: E731
+    # Each step: a bounded sample of the workload's rays (2^20 rays).
+    sample = 1 << 20 if kind == "reference" else 1 << 15
+    for w in range(args.warmup):
+        trace(rays[:sample])
+    times = []
+    for k in range(args.steps):
+        off = (k * sample) % (rays.shape[0] - sample + 1)
+        t0 = time.perf_counter()
+        trace(rays[off:off + sample])
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = sample * args.steps / total / 1e6
+    line = {
+        "impl": "reference", "metric": "closest-hit Mrays/s", "value": round(value, 4), "unit": "Mrays/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * total / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(args.layout),
+        "cpu_baseline": {"value": round(value, 4), "unit": "Mrays/s", "cores": threads, "kind": kind,
+                         "sample": f"{sample} rays per step of the 2^24-ray batch, BVHScene built once"},
+        "e2e": {"value": round(value, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(layout):
+    return {"workload": "ray-intersection: 2^24 rays x 1,048,576-triangle soup, closest hit",
+            "rays": NUM_RAYS, "triangles": NUM_TRIS,
+            "layout": {"bvh": "binary SAH BVH (reference bvh, bit-exact)",
+                       "qbvh": "4-wide collapse of the reference tree (bit-exact)"}[layout],
+            "l2": "inputs larger than L2 (512 MB of rays per step); no flush"}
+
+
+# ---------------------------------------------------------------- ours ------
+
+def run_ours(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+    from lightmetrica_b200 import native
+    from lightmetrica_b200.scene import Scene, soup_primitives
+    from lightmetrica_b200.workloads import random_rays, random_soup, rays_soa
+
+    pos, faces = random_soup(NUM_TRIS, seed=1)
+    rays = random_rays(NUM_RAYS, seed=2 + rank)
+    scene = Scene(args.layout)
+    scene.load(soup_primitives(pos, faces))
+    scene.configure({})
+    scene.build()
+    info = scene.info()
+
+    n = NUM_RAYS
+    soa = {k: torch.from_numpy(v).to(dev) for k, v in rays_soa(rays).items()}
+    hits = {"tri_id": torch.empty(n, dtype=torch.int32, device=dev)}
+    for k in ("t", "u", "v"):
+        hits[k] = torch.empty(n, dtype=torch.float32, device=dev)
+    R = native.RaysSoA(*[soa[k].data_ptr() for k in ("ox", "oy", "oz", "dx", "dy", "dz", "tmin", "tmax")])
+    H = native.HitsSoA(*[hits[k].data_ptr() for k in ("tri_id", "t", "u", "v")])
+    stream = torch.cuda.current_stream(dev)
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    L = native.lib()
+
+    # Reference work per ray (binary slab tests, TriAccel tests), counted on
+    # the device exactly as scene.bvh.cpp performs them; untimed.
+    counters = torch.zeros(2, dtype=torch.int64, device=dev)
+    native.check(L.lmgpu_intersect_counted(scene.handle, ctypes.byref(R), n, ctypes.byref(H),
+                                           ctypes.c_void_p(counters.data_ptr()), sptr))
+    scene.status(stream.cuda_stream)
+    node_tests, tri_tests = int(counters[0]), int(counters[1])
+    bytes_per_ray = RAY_IO_BYTES + NODE_BYTES * node_tests / n + TRI_BYTES * tri_tests / n
+    hit_frac = float((hits["tri_id"] >= 0).float().mean())
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    for _ in range(args.warmup):
+        native.check(L.lmgpu_intersect(scene.handle, ctypes.byref(R), n, ctypes.byref(H), sptr))
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for k in range(args.steps):
+        ev[k][0].record(stream)
+        native.check(L.lmgpu_intersect(scene.handle, ctypes.byref(R), n, ctypes.byref(H), sptr))
+        ev[k][1].record(stream)
+    t_end.record(stream)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    scene.status(stream.cuda_stream)
+    total_ms = t_start.elapsed_time(t_end)
+    launch_ms = [a.elapsed_time(b) for a, b in ev]
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t[0])
+    ms_per_step = total_ms / args.steps
+    value = world * n * args.steps / (total_ms / 1e3) / 1e6
+
+    # End to end through the host-buffer entry point: pinned AoS rays in, hit
+    # arrays out, copies inside the timed region.
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, scene, rays, hits, world, dev)
+
+    peak, peak_kind = measured_peaks()
+    avg_launch_ms = sum(launch_ms) / len(launch_ms)
+    achieved = bytes_per_ray * n / (avg_launch_ms / 1e3) / 1e9
+    traffic = load_traffic(args.layout)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, kind, cores, done, secs = cpu_reference_rate(pos, faces, rays)
+        cpu = {"value": round(rate, 4), "unit": "Mrays/s", "cores": cores, "kind": kind,
+               "sample": f"first {done} rays of the 2^24-ray batch ({secs:.1f} s), reference BVHScene built once"}
+
+    if rank == 0:
+        line = {
+            "metric": "closest-hit Mrays/s", "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded; no public scene exists for this workload)",
+            "config": dict(workload_config(args.layout), parallelism=f"replicas x{world}",
+                           hit_fraction=round(hit_frac, 4), bvh_nodes=info["num_nodes"], bvh_depth=info["max_depth"],
+                           build_seconds=round(info["build_seconds"], 3)),
+            "e2e": e2e,
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "bytes_per_ray": round(bytes_per_ray, 2),
+                         "node_tests_per_ray": round(node_tests / n, 3), "tri_tests_per_ray": round(tri_tests / n, 4)},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "kernel_ms": {"avg": round(avg_launch_ms, 4), "min": round(min(launch_ms), 4),
+                          "max": round(max(launch_ms), 4)},
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def run_e2e(args, scene, rays, hits, world, dev):
+    """Same metric through the host-buffer entry point lmgpu_intersect_host:
+    pinned AoS rays in, hit arrays out, copies inside the timed region."""
+    import torch
+    from lightmetrica_b200 import native
+    L = native.lib()
+    n = rays.shape[0]
+    rays_pinned = torch.from_numpy(rays).pin_memory()
+    out_id = torch.empty(n, dtype=torch.int32).pin_memory()
+    out_t = torch.empty(n, dtype=torch.float32).pin_memory()
+    out_u = torch.empty(n, dtype=torch.float32).pin_memory()
+    out_v = torch.empty(n, dtype=torch.float32).pin_memory()
+    e2e_steps = max(3, args.steps // 4)
+
+    def e2e_once():
+        native.check(L.lmgpu_intersect_host(scene.handle, rays_pinned.data_ptr(), n, out_id.data_ptr(),
+                                            out_t.data_ptr(), out_u.data_ptr(), out_v.data_ptr()))
+    e2e_once()
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_once()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t[0])
+    e2e_value = world * n * e2e_steps / e2e_s / 1e6
+    assert np.array_equal(out_id.numpy(), hits["tri_id"].cpu().numpy()), "host and device paths disagree"
+    return {"value": round(e2e_value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": n * 32,
+            "d2h_bytes_per_step": n * 16, "steps": e2e_steps}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

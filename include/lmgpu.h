@@ -1,0 +1,244 @@
+/*
+ * lmgpu.h — C ABI of the lightmetrica B200 path-tracing core.
+ *
+ * This is the drop-in boundary for lightmetrica's scene-accelerator slot and
+ * path-tracer bounce loop. A lightmetrica plugin (plugin.gpu.so) or any other
+ * host program builds a scene from world-space primitives, then issues
+ * intersection queries or whole renders. Plain C types only: no C++ or torch
+ * types cross this boundary, and no exceptions escape it.
+ *
+ * Conventions
+ *   - Every entry point returns an int status: LMGPU_OK (0) or a negative
+ *     LMGPU_ERR_* code; lmgpu_last_error() gives a message for the calling
+ *     thread.
+ *   - Handles are opaque and freed only by their destroy call.
+ *   - Caller buffers are borrowed for the duration of the call.
+ *   - A handle is used by one host thread at a time; independent handles may
+ *     run concurrently on separate CUDA streams.
+ *   - `stream` arguments are cudaStream_t passed as void* (NULL = legacy
+ *     default stream).
+ */
+#ifndef LMGPU_H
+#define LMGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LMGPU_ABI_VERSION 1
+
+/* ------------------------------------------------------------ status ---- */
+enum {
+    LMGPU_OK = 0,
+    LMGPU_ERR_INVALID = -1,        /* bad argument or scene description */
+    LMGPU_ERR_OOM = -2,            /* host or device allocation failed */
+    LMGPU_ERR_CUDA = -3,           /* a CUDA call failed */
+    LMGPU_ERR_STACK_OVERFLOW = -4, /* traversal stack exceeded (device flag) */
+    LMGPU_ERR_QUEUE_OVERFLOW = -5, /* wavefront queue exceeded (device flag) */
+    LMGPU_ERR_TIMEOUT = -6,        /* a bounded device wait gave up */
+    LMGPU_ERR_UNSUPPORTED = -7     /* feature not available for this scene */
+};
+
+/* ------------------------------------------------------------- scene ---- */
+
+/* Acceleration layouts. BVH2 reproduces the reference `bvh` scene
+ * (src/liblightmetrica/scene.bvh.cpp) exactly: same tree, same traversal
+ * order, same float arithmetic, hence bit-identical closest hits. */
+enum {
+    LMGPU_LAYOUT_BVH2 = 0,   /* binary, children-in-parent 64 B nodes */
+    LMGPU_LAYOUT_BVH4 = 1,   /* 4-wide collapse of the same tree, 128 B nodes */
+    LMGPU_LAYOUT_NAIVE = 2   /* brute force over all triangles (tiny scenes) */
+};
+
+/* BSDFs (reference diffuse.cpp, mirror.cpp, plugin.diffusemirror). */
+enum {
+    LMGPU_BSDF_DIFFUSE = 0,
+    LMGPU_BSDF_MIRROR = 1,
+    LMGPU_BSDF_DIFFUSE_MIRROR = 2,
+    LMGPU_BSDF_BLACK = 3
+};
+
+typedef struct LmgpuScene LmgpuScene;
+
+/* One lightmetrica Primitive (reference include/lightmetrica/primitive.h:39-60)
+ * with its TriangleMesh (trianglemesh.h:34-84). Vertices are in object space;
+ * `transform` is the primitive's 4x4 matrix, column-major like the
+ * reference's Math::Mat4 (NULL = identity) and is applied in the reference's
+ * float order. `num_faces` counts triangles (the reference's NumFaces()/3). */
+typedef struct {
+    const float* positions;     /* 3 * num_vertices */
+    const float* normals;       /* 3 * num_vertices, NULL = geometric normal */
+    const float* texcoords;     /* 2 * num_vertices, NULL = none */
+    const uint32_t* faces;      /* 3 * num_faces */
+    int32_t num_vertices;
+    int32_t num_faces;
+    const float* transform;     /* 16 floats or NULL */
+    int32_t material;           /* index into LmgpuSceneDesc.materials, -1 = black */
+    int32_t area_light;         /* index into LmgpuSceneDesc.area_lights, -1 = none */
+} LmgpuPrimitiveDesc;
+
+typedef struct {
+    int32_t type;               /* LMGPU_BSDF_* */
+    float reflectance[3];       /* R (diffuse_reflectance / specular_reflectance) */
+} LmgpuMaterialDesc;
+
+typedef struct {
+    float luminance[3];         /* reference light.area.cpp `luminance` (Le) */
+} LmgpuAreaLightDesc;
+
+typedef struct {
+    const LmgpuPrimitiveDesc* primitives;
+    int32_t num_primitives;
+    const LmgpuMaterialDesc* materials;
+    int32_t num_materials;
+    const LmgpuAreaLightDesc* area_lights;
+    int32_t num_area_lights;
+    int32_t has_env_light;      /* reference light.env.const.cpp */
+    float env_luminance[3];
+    /* Pinhole camera (reference perspectivecamera.cpp; view = LookAt). */
+    int32_t has_camera;
+    float camera_eye[3];
+    float camera_center[3];
+    float camera_up[3];
+    float camera_fovy_degrees;
+    int32_t film_width;
+    int32_t film_height;
+    int32_t layout;             /* LMGPU_LAYOUT_* */
+    int32_t build_threads;      /* host threads for the BVH build, 0 = all */
+} LmgpuSceneDesc;
+
+typedef struct {
+    int64_t num_triangles;
+    int64_t num_nodes;          /* binary BVH nodes (reference count) */
+    int64_t num_leaves;
+    int32_t max_depth;
+    int32_t layout;
+    int64_t device_bytes;       /* acceleration + geometry bytes in HBM */
+    double build_seconds;       /* host BVH build time */
+    float bounds_min[3];        /* Scene::GetAABBTriangles */
+    float bounds_max[3];
+} LmgpuSceneInfo;
+
+/* Replaces Scene::Load + Configure + Build (reference scene.h:47-191,
+ * scene.bvh.cpp:202-268): builds the accelerator on the host and uploads it. */
+int lmgpu_scene_create(const LmgpuSceneDesc* desc, LmgpuScene** out_scene);
+int lmgpu_scene_destroy(LmgpuScene* scene);
+int lmgpu_scene_info(const LmgpuScene* scene, LmgpuSceneInfo* info);
+
+/* Host-only build of the same accelerator, without any device work: fills
+ * `info` and, when `tri_order` is non-NULL (capacity >= triangles), the leaf
+ * triangle order (the reference's bvhTriIndices, scene.bvh.cpp:193). For
+ * validating the builder on machines without a GPU. */
+int lmgpu_scene_build_host(const LmgpuSceneDesc* desc, LmgpuSceneInfo* info,
+                           int32_t* tri_order, int64_t capacity);
+
+/* ------------------------------------------------------ intersection ---- */
+
+/* Ray batch, structure of arrays, DEVICE pointers (reference ray.h:37-45). */
+typedef struct {
+    const float* ox; const float* oy; const float* oz;
+    const float* dx; const float* dy; const float* dz;
+    const float* tmin; const float* tmax;
+} LmgpuRaysSoA;
+
+/* Closest-hit results, DEVICE pointers: triangle index in the reference's
+ * TriAccel numbering (primitive-major, scene.bvh.cpp:210-247) or -1, the hit
+ * distance t (the reference writes it to ray.maxT) and barycentrics (u, v). */
+typedef struct {
+    int32_t* tri_id; float* t; float* u; float* v;
+} LmgpuHitsSoA;
+
+/* Replaces BVHScene::IntersectTriangles for a batch (scene.bvh.cpp:390-448;
+ * TriAccel::Intersect triaccel.h:100-160). Asynchronous on `stream`. */
+int lmgpu_intersect(LmgpuScene* scene, const LmgpuRaysSoA* rays, int64_t n,
+                    LmgpuHitsSoA* hits, void* stream);
+
+/* Same query from HOST buffers: rays AoS (8 floats per ray: o.xyz, d.xyz,
+ * minT, maxT), outputs to host arrays (any may be NULL). Copies in, traces,
+ * copies out, synchronises. */
+int lmgpu_intersect_host(LmgpuScene* scene, const float* rays_aos, int64_t n,
+                         int32_t* tri_id, float* t, float* u, float* v);
+
+/* Any-hit visibility for shadow rays (reference RenderUtils::Visible,
+ * renderutils.cpp:58-70): occluded[i] = 1 if any triangle is hit within
+ * [tmin, tmax]. DEVICE pointers. */
+int lmgpu_occluded(LmgpuScene* scene, const LmgpuRaysSoA* rays, int64_t n,
+                   uint8_t* occluded, void* stream);
+
+/* Full hit record for tests of Scene::Intersect (scene.cpp:67-72,
+ * StoreIntersectionFromBarycentricCoords scene.cpp:101-149, emitter shapes
+ * primitives.cpp:214-238): HOST buffers; geom gets 17 floats per ray
+ * (p, gn, sn, ss, st, uv); kind[i] = 0 miss, 1 triangle, 2 environment. */
+int lmgpu_intersect_full_host(LmgpuScene* scene, const float* rays_aos, int64_t n,
+                              int32_t* tri_id, float* t, float* geom, int32_t* kind);
+
+/* ------------------------------------------------------------ render ---- */
+
+enum {
+    LMGPU_RENDER_PT = 0,         /* reference pathtrace.cpp  ("pt") */
+    LMGPU_RENDER_PT_DIRECT = 1,  /* reference pathtrace.direct.cpp ("pt.direct") */
+    LMGPU_RENDER_PT_MIS = 2      /* reference pathtrace.mis.cpp ("pt.mis") */
+};
+
+enum {
+    LMGPU_SAMPLING_STRATIFIED = 0, /* num_samples/(W*H) samples per pixel */
+    LMGPU_SAMPLING_UNIFORM = 1     /* raster uniform over the film, as the reference */
+};
+
+typedef struct {
+    int32_t technique;          /* LMGPU_RENDER_* */
+    int32_t rr_depth;           /* reference `rr_depth` (default 1, -1 = off) */
+    int32_t max_path_vertices;  /* reference `max_path_vertices` (-1 = unbounded) */
+    int32_t sampling;           /* LMGPU_SAMPLING_* */
+    uint64_t seed;
+    int64_t num_samples;        /* reference `num_samples`: total samples */
+    int64_t sample_offset;      /* first sample index (for splitting a budget) */
+    int32_t film_fp64;          /* accumulate the film in FP64 (oracle runs) */
+    int32_t wave_paths;         /* paths in flight per wave, 0 = automatic */
+} LmgpuRenderParams;
+
+typedef struct {
+    int64_t rays_traced;        /* closest-hit + shadow rays */
+    int64_t shadow_rays;
+    int64_t paths;
+    int32_t waves;
+    int32_t max_bounces_run;
+    double device_ms;           /* device time of the render (CUDA events) */
+} LmgpuRenderStats;
+
+/* Renders `num_samples` samples and writes the rescaled film (W*H*3 floats,
+ * row y = 0 first, reference HDRBitmapFilm layout) to a HOST buffer:
+ * the whole RenderProcessScheduler::Render (sched.mt.cpp:93-266) in one call. */
+int lmgpu_render(LmgpuScene* scene, const LmgpuRenderParams* params,
+                 float* film_host, LmgpuRenderStats* stats);
+
+/* Device variant: accumulates un-rescaled contributions into a DEVICE film
+ * (float, or double when film_fp64) on `stream`; the caller rescales by
+ * W*H/num_samples. No host synchronisation. */
+int lmgpu_render_device(LmgpuScene* scene, const LmgpuRenderParams* params,
+                        void* film_device, void* stream, LmgpuRenderStats* stats);
+
+/* ------------------------------------------------------------- misc ----- */
+const char* lmgpu_last_error(void);
+int lmgpu_abi_version(void);
+
+/* Reads and clears the scene's device status word after asynchronous calls
+ * (synchronises `stream`): traversal-stack or queue overflow and bounded-wait
+ * timeouts raised inside kernels come back here as LMGPU_ERR_* codes. */
+int lmgpu_scene_status(LmgpuScene* scene, void* stream);
+
+/* Measurement variant of lmgpu_intersect: additionally adds the number of
+ * binary-node slab tests and TriAccel tests of the batch to two DEVICE
+ * unsigned long long counters (the reference's per-ray work, counted the way
+ * scene.bvh.cpp:405-473 performs it). */
+int lmgpu_intersect_counted(LmgpuScene* scene, const LmgpuRaysSoA* rays, int64_t n,
+                            LmgpuHitsSoA* hits, unsigned long long* counters_device,
+                            void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LMGPU_H */

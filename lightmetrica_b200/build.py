@@ -1,0 +1,89 @@
+"""Builds the native core in-tree: lightmetrica_b200/_lib/liblmgpu.so.
+
+CUDA sources are compiled for sm_100a only
+(-gencode arch=compute_100a,code=sm_100a); the host BVH builder is compiled by
+the system g++ with -ffp-contract=off so that its float arithmetic rounds
+each operation separately, like the reference's float SSE build.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT_DIR = os.path.join(HERE, "_lib")
+OUT = os.path.join(OUT_DIR, "liblmgpu.so")
+BUILD_DIR = os.path.join(HERE, "_build")
+
+CU_SOURCES = ["api.cu", "pathtrace.cu"]
+CPP_SOURCES = ["builder.cpp"]
+HEADERS = ["layout.h", "builder.h", "internal.h", "scene.cuh", "trace.cuh", "trace4.cuh",
+           "shading.cuh", "rng.cuh", "pathtrace.cuh"]
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _nvcc():
+    cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    p = os.path.join(cuda, "bin", "nvcc")
+    return p if os.path.exists(p) else (shutil.which("nvcc") or "nvcc")
+
+
+def _cxx():
+    return "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else (shutil.which("g++") or "g++")
+
+
+def _stale(obj, deps):
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    return any(os.path.exists(d) and os.path.getmtime(d) > t for d in deps)
+
+
+def build(verbose: bool = False, ptxas_verbose: bool = False) -> str:
+    os.makedirs(OUT_DIR, exist_ok=True)
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(os.path.dirname(HERE), "include", "lmgpu.h")]
+    objs = []
+    procs = []
+    for src in CU_SOURCES:
+        s = os.path.join(CSRC, src)
+        if not os.path.exists(s):
+            continue
+        o = os.path.join(BUILD_DIR, src + ".o")
+        objs.append(o)
+        if _stale(o, [s] + hdrs):
+            cmd = [_nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
+                   "-Xcompiler", "-ffp-contract=off", "--expt-relaxed-constexpr",
+                   "-ccbin", _cxx(), "-c", s, "-o", o]
+            if ptxas_verbose:
+                cmd.insert(1, "-Xptxas=-v")
+            procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
+    for src in CPP_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD_DIR, src + ".o")
+        objs.append(o)
+        if _stale(o, [s] + hdrs):
+            cmd = [_cxx(), "-O2", "-std=c++17", "-fPIC", "-pthread", "-ffp-contract=off", "-fno-fast-math",
+                   "-c", s, "-o", o]
+            procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
+    for cmd, p in procs:
+        out, _ = p.communicate()
+        if verbose or ptxas_verbose or p.returncode != 0:
+            sys.stdout.write(out)
+        if p.returncode != 0:
+            raise RuntimeError("compile failed: " + " ".join(cmd))
+    if _stale(OUT, objs):
+        cmd = [_nvcc(), *ARCH, "-shared", "-ccbin", _cxx(), "-o", OUT, *objs, "-Xcompiler", "-pthread"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stdout.write(r.stdout + r.stderr)
+            raise RuntimeError("link failed")
+    return OUT
+
+
+if __name__ == "__main__":
+    print(build(verbose=True, ptxas_verbose="-v" in sys.argv))

@@ -1,0 +1,618 @@
+// C ABI: scene creation/upload and intersection queries.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/lmgpu.h"
+#include "builder.h"
+#include "internal.h"
+#include "trace.cuh"
+#include "trace4.cuh"
+
+namespace lmgpu {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int fail(int code, const std::string& msg)
+{
+    g_last_error = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what)
+{
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return LMGPU_ERR_CUDA;
+}
+
+int consume_status(LmgpuScene* s, cudaStream_t stream)
+{
+    int32_t st = 0;
+    LMGPU_CUDA_TRY(cudaMemcpyAsync(&st, s->d_status, sizeof(st), cudaMemcpyDeviceToHost, stream));
+    LMGPU_CUDA_TRY(cudaStreamSynchronize(stream));
+    if (st == 0) return LMGPU_OK;
+    LMGPU_CUDA_TRY(cudaMemsetAsync(s->d_status, 0, sizeof(int32_t), stream));
+    if (st & STATUS_STACK_OVERFLOW) return fail(LMGPU_ERR_STACK_OVERFLOW, "traversal stack bound exceeded");
+    if (st & STATUS_QUEUE_OVERFLOW) return fail(LMGPU_ERR_QUEUE_OVERFLOW, "wavefront queue bound exceeded");
+    if (st & STATUS_TIMEOUT) return fail(LMGPU_ERR_TIMEOUT, "bounded device wait gave up");
+    return fail(LMGPU_ERR_CUDA, "unknown device status");
+}
+
+namespace {
+
+template <class T>
+int upload(LmgpuScene* s, const std::vector<T>& v, const T** out)
+{
+    *out = nullptr;
+    if (v.empty()) return LMGPU_OK;
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, v.size() * sizeof(T));
+    if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? fail(LMGPU_ERR_OOM, "device allocation failed") : cuda_fail(e, "cudaMalloc");
+    s->allocations.push_back(p);
+    LMGPU_CUDA_TRY(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    *out = static_cast<const T*>(p);
+    return LMGPU_OK;
+}
+
+// ---- camera matrices (reference math.transform.inl:88-113, perspectivecamera.cpp:97-160)
+bool mat_inverse(const double* m, double* inv)
+{
+    // Gauss-Jordan on a row-major copy.
+    double a[4][8];
+    for (int r = 0; r < 4; r++)
+        for (int c = 0; c < 4; c++) { a[r][c] = m[4 * c + r]; a[r][4 + c] = r == c ? 1.0 : 0.0; }
+    for (int c = 0; c < 4; c++) {
+        int piv = c;
+        for (int r = c + 1; r < 4; r++) if (std::fabs(a[r][c]) > std::fabs(a[piv][c])) piv = r;
+        if (a[piv][c] == 0.0) return false;
+        if (piv != c) for (int k = 0; k < 8; k++) std::swap(a[c][k], a[piv][k]);
+        const double d = a[c][c];
+        for (int k = 0; k < 8; k++) a[c][k] /= d;
+        for (int r = 0; r < 4; r++) {
+            if (r == c) continue;
+            const double f = a[r][c];
+            for (int k = 0; k < 8; k++) a[r][k] -= f * a[c][k];
+        }
+    }
+    for (int r = 0; r < 4; r++)
+        for (int c = 0; c < 4; c++) inv[4 * c + r] = a[r][4 + c];
+    return true;
+}
+
+void normalize3(double* v)
+{
+    const double l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    for (int i = 0; i < 3; i++) v[i] /= l;
+}
+
+bool setup_camera(const LmgpuSceneDesc& d, CameraGpu& cam)
+{
+    std::memset(&cam, 0, sizeof(cam));
+    if (!d.has_camera) return true;
+    if (d.film_width <= 0 || d.film_height <= 0 || !(d.camera_fovy_degrees > 0.0f)) return false;
+    double eye[3], ctr[3], up[3];
+    for (int i = 0; i < 3; i++) { eye[i] = d.camera_eye[i]; ctr[i] = d.camera_center[i]; up[i] = d.camera_up[i]; }
+    // LookAt: f = normalize(center - eye), s = normalize(f x up), u = s x f
+    double f[3] = { ctr[0] - eye[0], ctr[1] - eye[1], ctr[2] - eye[2] };
+    normalize3(f);
+    double u[3] = { up[0], up[1], up[2] };
+    normalize3(u);
+    double s[3] = { f[1] * u[2] - f[2] * u[1], f[2] * u[0] - f[0] * u[2], f[0] * u[1] - f[1] * u[0] };
+    normalize3(s);
+    u[0] = s[1] * f[2] - s[2] * f[1]; u[1] = s[2] * f[0] - s[0] * f[2]; u[2] = s[0] * f[1] - s[1] * f[0];
+    const double view[16] = { s[0], u[0], -f[0], 0, s[1], u[1], -f[1], 0, s[2], u[2], -f[2], 0,
+                              -(s[0] * eye[0] + s[1] * eye[1] + s[2] * eye[2]),
+                              -(u[0] * eye[0] + u[1] * eye[1] + u[2] * eye[2]),
+                              (f[0] * eye[0] + f[1] * eye[1] + f[2] * eye[2]), 1 };
+    const double aspect = double(d.film_width) / double(d.film_height);
+    const double rad = double(d.camera_fovy_degrees) * 3.14159265358979323846 / 180.0;
+    const double t = std::tan(rad / 2.0);
+    const double zn = 1.0, zf = 1000.0;
+    const double proj[16] = { 1.0 / (aspect * t), 0, 0, 0, 0, 1.0 / t, 0, 0,
+                              0, 0, -(zf + zn) / (zf - zn), -1, 0, 0, -(2.0 * zf * zn) / (zf - zn), 0 };
+    double iview[16], iproj[16];
+    if (!mat_inverse(view, iview) || !mat_inverse(proj, iproj)) return false;
+    for (int i = 0; i < 16; i++) {
+        cam.view[i] = float(view[i]); cam.inv_view[i] = float(iview[i]);
+        cam.proj[i] = float(proj[i]); cam.inv_proj[i] = float(iproj[i]);
+    }
+    for (int i = 0; i < 3; i++) cam.position[i] = float(iview[12 + i]);
+    // Sensor area at distance 1 (perspectivecamera.cpp:145-156).
+    auto unproj = [&](double x, double y, double* o) {
+        double v[4] = { x, y, 0, 1 }, w[4];
+        for (int r = 0; r < 4; r++) w[r] = iproj[r] * v[0] + iproj[4 + r] * v[1] + iproj[8 + r] * v[2] + iproj[12 + r] * v[3];
+        for (int k = 0; k < 3; k++) o[k] = w[k] / w[3];
+        for (int k = 0; k < 3; k++) o[k] = o[k] / o[2];
+    };
+    double p1[3], p2[3];
+    unproj(-1, -1, p1);
+    unproj(1, 1, p2);
+    const double A = (p2[0] - p1[0]) * (p2[1] - p1[1]);
+    cam.inv_A = float(1.0 / A);
+    cam.width = d.film_width;
+    cam.height = d.film_height;
+    cam.valid = 1;
+    return true;
+}
+
+int create_impl(const LmgpuSceneDesc* desc, LmgpuScene** out)
+{
+    if (!desc || !out) return fail(LMGPU_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (desc->num_primitives < 0 || (desc->num_primitives > 0 && !desc->primitives))
+        return fail(LMGPU_ERR_INVALID, "bad primitive list");
+    if (desc->layout < LMGPU_LAYOUT_BVH2 || desc->layout > LMGPU_LAYOUT_NAIVE)
+        return fail(LMGPU_ERR_INVALID, "unknown layout");
+    for (int i = 0; i < desc->num_primitives; i++) {
+        const auto& p = desc->primitives[i];
+        if (p.material >= desc->num_materials || p.area_light >= desc->num_area_lights)
+            return fail(LMGPU_ERR_INVALID, "primitive references a missing material or light");
+        if (p.positions && p.num_vertices > 0)
+            for (int64_t k = 0; k < 3 * (int64_t)p.num_vertices; k++)
+                if (!std::isfinite(p.positions[k])) return fail(LMGPU_ERR_INVALID, "non-finite vertex position");
+    }
+    for (int i = 0; i < desc->num_materials; i++)
+        if (desc->materials[i].type < LMGPU_BSDF_DIFFUSE || desc->materials[i].type > LMGPU_BSDF_BLACK)
+            return fail(LMGPU_ERR_INVALID, "unknown BSDF type");
+
+    std::vector<PrimitiveInput> prims(desc->num_primitives);
+    for (int i = 0; i < desc->num_primitives; i++) {
+        const auto& p = desc->primitives[i];
+        prims[i] = PrimitiveInput{ p.positions, p.normals, p.texcoords, p.faces, p.num_vertices, p.num_faces, p.transform };
+    }
+    BuiltScene b;
+    std::string err;
+    try {
+        err = build_scene(prims, desc->build_threads, desc->layout != LMGPU_LAYOUT_NAIVE, b);
+    } catch (const std::bad_alloc&) {
+        return fail(LMGPU_ERR_OOM, "host allocation failed during the BVH build");
+    }
+    if (!err.empty()) return fail(LMGPU_ERR_INVALID, err);
+
+    CameraGpu cam;
+    if (!setup_camera(*desc, cam)) return fail(LMGPU_ERR_INVALID, "invalid camera");
+
+    LmgpuScene* s = new (std::nothrow) LmgpuScene;
+    if (!s) return fail(LMGPU_ERR_OOM, "host allocation failed");
+    LMGPU_CUDA_TRY(cudaGetDevice(&s->device));
+    DeviceScene& d = s->dev;
+    std::memset(&d, 0, sizeof(d));
+    d.layout = desc->layout;
+    d.num_tris = b.num_tris;
+    d.root_ref = b.bvh2_root;
+    d.root_ref4 = b.bvh4_root;
+    d.stack_cap = 2 * b.max_depth + 4;
+    std::memcpy(d.root_box, b.root_box, sizeof(d.root_box));
+    d.cam = cam;
+
+    int rc = LMGPU_OK;
+    auto up = [&](auto& vec, auto** dst) { if (rc == LMGPU_OK) rc = upload(s, vec, dst); };
+    up(b.tris, &d.tris);
+    up(b.bvh2, &d.bvh2);
+    up(b.bvh4, &d.bvh4);
+    std::vector<TriRecord> by_id;
+    if (desc->layout == LMGPU_LAYOUT_NAIVE) {
+        by_id.resize(b.tris.size());
+        for (auto& t : b.tris) by_id[t.tri_id] = t;
+        up(by_id, &d.tris_by_id);
+    }
+    up(b.positions, &d.vpos);
+    up(b.normals, &d.vnrm);
+    up(b.texcoords, &d.vuv);
+    up(b.tri_vidx, &d.tri_vidx);
+    up(b.tri_prim, &d.tri_prim);
+
+    std::vector<int32_t> pm(desc->num_primitives), pl(desc->num_primitives);
+    for (int i = 0; i < desc->num_primitives; i++) {
+        pm[i] = desc->primitives[i].material;
+        pl[i] = desc->primitives[i].area_light;
+    }
+    up(pm, &d.prim_material);
+    up(pl, &d.prim_light);
+    std::vector<float4> mats(std::max(1, desc->num_materials));
+    for (int i = 0; i < desc->num_materials; i++) {
+        const auto& m = desc->materials[i];
+        float type_bits;
+        std::memcpy(&type_bits, &m.type, sizeof(float));
+        mats[i] = make_float4(m.reflectance[0], m.reflectance[1], m.reflectance[2], type_bits);
+    }
+    up(mats, &d.materials);
+    d.num_materials = desc->num_materials;
+
+    // Area lights: triangle-area CDF per light in primitive order
+    // (light.area.cpp:109-144).
+    std::vector<AreaLightGpu> lights(desc->num_area_lights);
+    std::vector<float> cdf;
+    std::vector<int32_t> ltris;
+    for (int li = 0; li < desc->num_area_lights; li++) {
+        AreaLightGpu& L = lights[li];
+        std::memset(&L, 0, sizeof(L));
+        for (int c = 0; c < 3; c++) L.Le[c] = desc->area_lights[li].luminance[c];
+        L.cdf_begin = static_cast<int32_t>(cdf.size());
+        std::vector<double> acc{ 0.0 };
+        for (int64_t t = 0; t < b.num_tris; t++) {
+            if (desc->primitives[b.tri_prim[t]].area_light != li) continue;
+            const float* p1 = &b.positions[3 * (size_t)b.tri_vidx[3 * t]];
+            const float* p2 = &b.positions[3 * (size_t)b.tri_vidx[3 * t + 1]];
+            const float* p3 = &b.positions[3 * (size_t)b.tri_vidx[3 * t + 2]];
+            double e1[3], e2[3];
+            for (int c = 0; c < 3; c++) { e1[c] = double(p2[c]) - p1[c]; e2[c] = double(p3[c]) - p1[c]; }
+            const double cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2], cz = e1[0] * e2[1] - e1[1] * e2[0];
+            acc.push_back(acc.back() + 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz));
+            ltris.push_back(static_cast<int32_t>(t));
+        }
+        const double area = acc.back();
+        if (!(area > 0.0)) return fail(LMGPU_ERR_INVALID, "area light without area");
+        for (double v : acc) cdf.push_back(float(v / area));
+        L.num_tris = static_cast<int32_t>(acc.size() - 1);
+        L.area = float(area);
+        L.inv_area = float(1.0 / area);
+    }
+    up(lights, &d.area_lights);
+    up(cdf, &d.light_cdf);
+    up(ltris, &d.light_tris);
+    d.num_area_lights = desc->num_area_lights;
+    d.has_env = desc->has_env_light ? 1 : 0;
+    d.num_lights = d.num_area_lights + d.has_env;
+    if (d.has_env) {
+        // Bounding sphere of triangles + camera (light.env.const.cpp:90-97, scene.cpp:58-65).
+        float mn[3], mx[3];
+        for (int c = 0; c < 3; c++) { mn[c] = b.bounds.mn[c]; mx[c] = b.bounds.mx[c]; }
+        if (cam.valid)
+            for (int c = 0; c < 3; c++) { mn[c] = std::min(mn[c], cam.position[c]); mx[c] = std::max(mx[c], cam.position[c]); }
+        double r2 = 0;
+        for (int c = 0; c < 3; c++) {
+            d.env_center[c] = float((double(mx[c]) + mn[c]) / 2.0);
+            const double dd = double(d.env_center[c]) - mx[c];
+            r2 += dd * dd;
+            d.env_Le[c] = desc->env_luminance[c];
+        }
+        d.env_radius = float(std::sqrt(r2));
+        d.env_inv_area = float(1.0 / (4.0 * 3.14159265358979323846 * r2));
+    }
+    if (rc != LMGPU_OK) { lmgpu_scene_destroy(s); return rc; }
+
+    void* st = nullptr;
+    cudaError_t e = cudaMalloc(&st, sizeof(int32_t));
+    if (e != cudaSuccess) { lmgpu_scene_destroy(s); return cuda_fail(e, "cudaMalloc(status)"); }
+    s->allocations.push_back(st);
+    s->d_status = static_cast<int32_t*>(st);
+    LMGPU_CUDA_TRY(cudaMemset(s->d_status, 0, sizeof(int32_t)));
+
+    LmgpuSceneInfo& info = s->info;
+    info.num_triangles = b.num_tris;
+    info.num_nodes = static_cast<int64_t>(b.nodes.size());
+    info.num_leaves = b.num_leaves;
+    info.max_depth = b.max_depth;
+    info.layout = desc->layout;
+    info.build_seconds = b.build_seconds;
+    int64_t bytes = 0;
+    bytes += (int64_t)b.tris.size() * sizeof(TriRecord);
+    bytes += (desc->layout == LMGPU_LAYOUT_BVH4 ? (int64_t)b.bvh4.size() * sizeof(Bvh4Node) : (int64_t)b.bvh2.size() * sizeof(Bvh2Node));
+    info.device_bytes = bytes;
+    for (int c = 0; c < 3; c++) { info.bounds_min[c] = b.bounds.mn[c]; info.bounds_max[c] = b.bounds.mx[c]; }
+    *out = s;
+    return LMGPU_OK;
+}
+
+// ------------------------------------------------------------- kernels ----
+
+// Ray source: SoA arrays (device API) or AoS records of 8 floats
+// (o.xyz, d.xyz, minT, maxT; the host-buffer API), read with two 16 B loads.
+struct RaySrc {
+    LmgpuRaysSoA soa;
+    const float4* aos;   // non-null selects AoS
+};
+
+__device__ __forceinline__ RayIn load_ray(const RaySrc& R, int64_t i)
+{
+    RayIn in;
+    if (R.aos) {
+        const float4 a = __ldg(R.aos + 2 * i), b = __ldg(R.aos + 2 * i + 1);
+        in.o[0] = a.x; in.o[1] = a.y; in.o[2] = a.z;
+        in.d[0] = a.w; in.d[1] = b.x; in.d[2] = b.y;
+        in.tmin = b.z; in.tmax = b.w;
+        return in;
+    }
+    in.o[0] = __ldg(R.soa.ox + i); in.o[1] = __ldg(R.soa.oy + i); in.o[2] = __ldg(R.soa.oz + i);
+    in.d[0] = __ldg(R.soa.dx + i); in.d[1] = __ldg(R.soa.dy + i); in.d[2] = __ldg(R.soa.dz + i);
+    in.tmin = __ldg(R.soa.tmin + i); in.tmax = __ldg(R.soa.tmax + i);
+    return in;
+}
+
+template <int LAYOUT, bool ANY_HIT, int STACK>
+__device__ __forceinline__ bool trace_one(const DeviceScene& s, TraversalRay& r, Hit& h, int2* stack, TraceStats* st)
+{
+    if (s.num_tris == 0) { h.tri = -1; return true; }   // empty scene: no node arrays exist
+    if (LAYOUT == LMGPU_LAYOUT_BVH2)
+        return trace_bvh2<ANY_HIT>(s.bvh2, s.tris, s.root_ref, s.root_box, r, h, stack, STACK, st);
+    if (LAYOUT == LMGPU_LAYOUT_BVH4)
+        return trace_bvh4<ANY_HIT>(s.bvh4, s.tris, s.root_ref4, s.root_box, r, h, stack, STACK, st);
+    trace_naive<ANY_HIT>(s.tris_by_id, s.num_tris, r, h, st);
+    return true;
+}
+
+template <int LAYOUT, int STACK, bool STATS>
+__global__ void __launch_bounds__(128) k_intersect(const DeviceScene s, const RaySrc rays, int64_t n,
+                                                   const LmgpuHitsSoA hits, int32_t* status,
+                                                   unsigned long long* counters)
+{
+    int2 stack[STACK];
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    TraceStats st{ 0, 0 };
+    if (i < n) {
+        TraversalRay r;
+        setup_ray(r, load_ray(rays, i));
+        Hit h;
+        const bool ok = trace_one<LAYOUT, false, STACK>(s, r, h, stack, STATS ? &st : nullptr);
+        if (!ok) { atomicOr(status, STATUS_STACK_OVERFLOW); h.tri = -1; }
+        const bool hit = h.tri >= 0;
+        if (hits.tri_id) hits.tri_id[i] = h.tri;
+        if (hits.t) hits.t[i] = hit ? h.t : 0.0f;
+        if (hits.u) hits.u[i] = hit ? h.u : 0.0f;
+        if (hits.v) hits.v[i] = hit ? h.v : 0.0f;
+    }
+    if (STATS) {
+        unsigned long long a = st.nodes, b = st.tris;
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, o);
+            b += __shfl_down_sync(0xffffffffu, b, o);
+        }
+        if ((threadIdx.x & 31) == 0) { atomicAdd(counters, a); atomicAdd(counters + 1, b); }
+    }
+}
+
+template <int LAYOUT, int STACK>
+__global__ void __launch_bounds__(128) k_occluded(const DeviceScene s, const RaySrc rays, int64_t n,
+                                                  uint8_t* occluded, int32_t* status)
+{
+    int2 stack[STACK];
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    TraversalRay r;
+    setup_ray(r, load_ray(rays, i));
+    Hit h;
+    const bool ok = trace_one<LAYOUT, true, STACK>(s, r, h, stack, nullptr);
+    if (!ok) atomicOr(status, STATUS_STACK_OVERFLOW);
+    occluded[i] = h.tri >= 0 ? 1 : 0;
+}
+
+template <int STACK>
+int launch_intersect_stack(LmgpuScene* sc, const RaySrc& rays, int64_t n, const LmgpuHitsSoA& hits,
+                           cudaStream_t stream, unsigned long long* counters)
+{
+    const int threads = 128;
+    const int64_t blocks = (n + threads - 1) / threads;
+    const DeviceScene& s = sc->dev;
+    if (counters) {
+        switch (s.layout) {
+        case LMGPU_LAYOUT_BVH2: k_intersect<LMGPU_LAYOUT_BVH2, STACK, true><<<blocks, threads, 0, stream>>>(s, rays, n, hits, sc->d_status, counters); break;
+        case LMGPU_LAYOUT_BVH4: k_intersect<LMGPU_LAYOUT_BVH4, STACK, true><<<blocks, threads, 0, stream>>>(s, rays, n, hits, sc->d_status, counters); break;
+        default: k_intersect<LMGPU_LAYOUT_NAIVE, 1, true><<<blocks, threads, 0, stream>>>(s, rays, n, hits, sc->d_status, counters); break;
+        }
+    } else {
+        switch (s.layout) {
+        case LMGPU_LAYOUT_BVH2: k_intersect<LMGPU_LAYOUT_BVH2, STACK, false><<<blocks, threads, 0, stream>>>(s, rays, n, hits, sc->d_status, nullptr); break;
+        case LMGPU_LAYOUT_BVH4: k_intersect<LMGPU_LAYOUT_BVH4, STACK, false><<<blocks, threads, 0, stream>>>(s, rays, n, hits, sc->d_status, nullptr); break;
+        default: k_intersect<LMGPU_LAYOUT_NAIVE, 1, false><<<blocks, threads, 0, stream>>>(s, rays, n, hits, sc->d_status, nullptr); break;
+        }
+    }
+    LMGPU_CUDA_TRY(cudaGetLastError());
+    return LMGPU_OK;
+}
+
+int launch_intersect(LmgpuScene* sc, const RaySrc& rays, int64_t n, const LmgpuHitsSoA& hits,
+                     cudaStream_t stream, unsigned long long* counters)
+{
+    if (n == 0) return LMGPU_OK;
+    const int cap = sc->dev.stack_cap;
+    if (cap <= 32) return launch_intersect_stack<32>(sc, rays, n, hits, stream, counters);
+    if (cap <= 64) return launch_intersect_stack<64>(sc, rays, n, hits, stream, counters);
+    if (cap <= 128) return launch_intersect_stack<128>(sc, rays, n, hits, stream, counters);
+    if (cap <= 256) return launch_intersect_stack<256>(sc, rays, n, hits, stream, counters);
+    return fail(LMGPU_ERR_UNSUPPORTED, "BVH deeper than the largest compiled traversal stack (256)");
+}
+
+template <int STACK>
+int launch_occluded_stack(LmgpuScene* sc, const RaySrc& rays, int64_t n, uint8_t* occ, cudaStream_t stream)
+{
+    const int threads = 128;
+    const int64_t blocks = (n + threads - 1) / threads;
+    const DeviceScene& s = sc->dev;
+    switch (s.layout) {
+    case LMGPU_LAYOUT_BVH2: k_occluded<LMGPU_LAYOUT_BVH2, STACK><<<blocks, threads, 0, stream>>>(s, rays, n, occ, sc->d_status); break;
+    case LMGPU_LAYOUT_BVH4: k_occluded<LMGPU_LAYOUT_BVH4, STACK><<<blocks, threads, 0, stream>>>(s, rays, n, occ, sc->d_status); break;
+    default: k_occluded<LMGPU_LAYOUT_NAIVE, 1><<<blocks, threads, 0, stream>>>(s, rays, n, occ, sc->d_status); break;
+    }
+    LMGPU_CUDA_TRY(cudaGetLastError());
+    return LMGPU_OK;
+}
+
+}  // namespace
+
+// Exposed for the measurement path (traversal counters).
+int ensure_host_pipeline(LmgpuScene* sc)
+{
+    HostPipeline& hp = sc->pipe;
+    if (hp.ready) return LMGPU_OK;
+    hp.chunk = int64_t(1) << 20;   // 1M rays: 32 MB in, 16 MB out per stage
+    for (int k = 0; k < 2; k++) {
+        LMGPU_CUDA_TRY(cudaStreamCreateWithFlags(&hp.stream[k], cudaStreamNonBlocking));
+        void* p = nullptr;
+        LMGPU_CUDA_TRY(cudaMalloc(&p, (size_t)hp.chunk * 12 * sizeof(float)));
+        sc->allocations.push_back(p);
+        hp.rays[k] = static_cast<float*>(p);
+        hp.hits[k] = hp.rays[k] + 8 * hp.chunk;
+    }
+    hp.ready = true;
+    return LMGPU_OK;
+}
+
+RaySrc soa_src(const LmgpuRaysSoA& r)
+{
+    RaySrc s;
+    s.soa = r;
+    s.aos = nullptr;
+    return s;
+}
+
+}  // namespace lmgpu
+
+using namespace lmgpu;
+
+extern "C" {
+
+int lmgpu_abi_version(void) { return LMGPU_ABI_VERSION; }
+
+const char* lmgpu_last_error(void) { return g_last_error.c_str(); }
+
+int lmgpu_scene_create(const LmgpuSceneDesc* desc, LmgpuScene** out_scene)
+{
+    try {
+        return create_impl(desc, out_scene);
+    } catch (const std::bad_alloc&) {
+        return fail(LMGPU_ERR_OOM, "host allocation failed");
+    } catch (...) {
+        return fail(LMGPU_ERR_INVALID, "unexpected exception during scene creation");
+    }
+}
+
+int lmgpu_scene_destroy(LmgpuScene* scene)
+{
+    if (!scene) return LMGPU_OK;
+    if (scene->pipe.ready)
+        for (int k = 0; k < 2; k++) cudaStreamDestroy(scene->pipe.stream[k]);
+    for (void* p : scene->allocations) cudaFree(p);
+    delete scene;
+    return LMGPU_OK;
+}
+
+int lmgpu_scene_info(const LmgpuScene* scene, LmgpuSceneInfo* info)
+{
+    if (!scene || !info) return fail(LMGPU_ERR_INVALID, "null argument");
+    *info = scene->info;
+    return LMGPU_OK;
+}
+
+int lmgpu_intersect(LmgpuScene* scene, const LmgpuRaysSoA* rays, int64_t n, LmgpuHitsSoA* hits, void* stream)
+{
+    if (!scene || !rays || !hits || n < 0) return fail(LMGPU_ERR_INVALID, "null argument or negative count");
+    if (n > 0 && (!rays->ox || !rays->oy || !rays->oz || !rays->dx || !rays->dy || !rays->dz || !rays->tmin || !rays->tmax))
+        return fail(LMGPU_ERR_INVALID, "null ray array");
+    return launch_intersect(scene, soa_src(*rays), n, *hits, static_cast<cudaStream_t>(stream), nullptr);
+}
+
+int lmgpu_occluded(LmgpuScene* scene, const LmgpuRaysSoA* rays, int64_t n, uint8_t* occluded, void* stream)
+{
+    if (!scene || !rays || !occluded || n < 0) return fail(LMGPU_ERR_INVALID, "null argument or negative count");
+    if (n == 0) return LMGPU_OK;
+    const int cap = scene->dev.stack_cap;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const RaySrc src = soa_src(*rays);
+    if (cap <= 32) return launch_occluded_stack<32>(scene, src, n, occluded, st);
+    if (cap <= 64) return launch_occluded_stack<64>(scene, src, n, occluded, st);
+    if (cap <= 128) return launch_occluded_stack<128>(scene, src, n, occluded, st);
+    if (cap <= 256) return launch_occluded_stack<256>(scene, src, n, occluded, st);
+    return fail(LMGPU_ERR_UNSUPPORTED, "BVH deeper than the largest compiled traversal stack (256)");
+}
+
+int lmgpu_intersect_host(LmgpuScene* scene, const float* rays_aos, int64_t n, int32_t* tri_id, float* t, float* u, float* v)
+{
+    if (!scene || (n > 0 && !rays_aos) || n < 0) return fail(LMGPU_ERR_INVALID, "null argument or negative count");
+    if (n == 0) return LMGPU_OK;
+    // Chunked two-stream pipeline: the H2D copy of chunk c+1 and the D2H copy
+    // of chunk c-1 overlap the traversal of chunk c. Staging buffers are
+    // cached in the scene and grown on demand.
+    int rc = ensure_host_pipeline(scene);
+    if (rc != LMGPU_OK) return rc;
+    HostPipeline& hp = scene->pipe;
+    const int64_t chunk = hp.chunk;
+    const int64_t nchunks = (n + chunk - 1) / chunk;
+    for (int64_t c = 0; c < nchunks && rc == LMGPU_OK; c++) {
+        const int k = static_cast<int>(c & 1);
+        cudaStream_t st = hp.stream[k];
+        const int64_t b = c * chunk, m = std::min(chunk, n - b);
+        float* dr = hp.rays[k];
+        float* dh = hp.hits[k];
+        cudaError_t e = cudaMemcpyAsync(dr, rays_aos + 8 * b, (size_t)m * 8 * sizeof(float), cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) { rc = cuda_fail(e, "cudaMemcpyAsync(rays)"); break; }
+        RaySrc src;
+        std::memset(&src, 0, sizeof(src));
+        src.aos = reinterpret_cast<const float4*>(dr);
+        LmgpuHitsSoA H{ reinterpret_cast<int32_t*>(dh), dh + chunk, dh + 2 * chunk, dh + 3 * chunk };
+        rc = launch_intersect(scene, src, m, H, st, nullptr);
+        if (rc != LMGPU_OK) break;
+        void* outs[4] = { tri_id, t, u, v };
+        for (int a = 0; a < 4 && rc == LMGPU_OK; a++) {
+            if (!outs[a]) continue;
+            e = cudaMemcpyAsync(static_cast<char*>(outs[a]) + 4 * b, dh + a * chunk, (size_t)m * 4, cudaMemcpyDeviceToHost, st);
+            if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemcpyAsync(hits)");
+        }
+    }
+    for (int k = 0; k < 2; k++) {
+        cudaError_t e = cudaStreamSynchronize(hp.stream[k]);
+        if (e != cudaSuccess && rc == LMGPU_OK) rc = cuda_fail(e, "cudaStreamSynchronize");
+    }
+    if (rc == LMGPU_OK) rc = consume_status(scene, hp.stream[0]);
+    return rc;
+}
+
+// Traversal counters (binary slab tests, TriAccel tests) summed over a batch;
+// counters must point to 2 device unsigned long long values (not cleared).
+int lmgpu_intersect_counted(LmgpuScene* scene, const LmgpuRaysSoA* rays, int64_t n, LmgpuHitsSoA* hits,
+                            unsigned long long* counters_device, void* stream)
+{
+    if (!scene || !rays || !hits || !counters_device || n < 0) return fail(LMGPU_ERR_INVALID, "null argument");
+    return launch_intersect(scene, soa_src(*rays), n, *hits, static_cast<cudaStream_t>(stream), counters_device);
+}
+
+// Host-only build (no device work): info and, optionally, the leaf triangle
+// order (the reference's bvhTriIndices, scene.bvh.cpp:193).
+int lmgpu_scene_build_host(const LmgpuSceneDesc* desc, LmgpuSceneInfo* info, int32_t* tri_order, int64_t capacity)
+{
+    if (!desc || !info) return fail(LMGPU_ERR_INVALID, "null argument");
+    std::vector<PrimitiveInput> prims(desc->num_primitives);
+    for (int i = 0; i < desc->num_primitives; i++) {
+        const auto& p = desc->primitives[i];
+        prims[i] = PrimitiveInput{ p.positions, p.normals, p.texcoords, p.faces, p.num_vertices, p.num_faces, p.transform };
+    }
+    BuiltScene b;
+    std::string err;
+    try {
+        err = build_scene(prims, desc->build_threads, desc->layout != LMGPU_LAYOUT_NAIVE, b);
+    } catch (const std::bad_alloc&) {
+        return fail(LMGPU_ERR_OOM, "host allocation failed during the BVH build");
+    }
+    if (!err.empty()) return fail(LMGPU_ERR_INVALID, err);
+    std::memset(info, 0, sizeof(*info));
+    info->num_triangles = b.num_tris;
+    info->num_nodes = static_cast<int64_t>(b.nodes.size());
+    info->num_leaves = b.num_leaves;
+    info->max_depth = b.max_depth;
+    info->layout = desc->layout;
+    info->build_seconds = b.build_seconds;
+    info->device_bytes = (int64_t)b.tris.size() * sizeof(TriRecord) +
+                         (desc->layout == LMGPU_LAYOUT_BVH4 ? (int64_t)b.bvh4.size() * sizeof(Bvh4Node)
+                                                            : (int64_t)b.bvh2.size() * sizeof(Bvh2Node));
+    for (int c = 0; c < 3; c++) { info->bounds_min[c] = b.bounds.mn[c]; info->bounds_max[c] = b.bounds.mx[c]; }
+    if (tri_order) {
+        if (capacity < b.num_tris) return fail(LMGPU_ERR_INVALID, "tri_order capacity too small");
+        std::memcpy(tri_order, b.tri_order.data(), (size_t)b.num_tris * sizeof(int32_t));
+    }
+    return LMGPU_OK;
+}
+
+// Status word of the last asynchronous calls on this scene (synchronises `stream`).
+int lmgpu_scene_status(LmgpuScene* scene, void* stream)
+{
+    if (!scene) return fail(LMGPU_ERR_INVALID, "null scene");
+    return consume_status(scene, static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

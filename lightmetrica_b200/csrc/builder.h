@@ -1,0 +1,68 @@
+// Host-side scene builder: world-space triangles, TriAccel records and the
+// binned-SAH BVH of the reference's `bvh` scene, flattened into the device
+// layouts of layout.h.
+#pragma once
+#include <stdint.h>
+#include <string>
+#include <vector>
+#include "layout.h"
+
+namespace lmgpu {
+
+struct HostAabb {
+    float mn[3], mx[3];
+};
+
+// Binary BVH node as built (reference BVHNode, scene.bvh.cpp:35-73).
+struct BuildNode {
+    HostAabb bound;
+    int32_t left = -1, right = -1;  // node indices (internal)
+    int32_t begin = 0, end = 0;     // triangle range in tri_order (leaf)
+    int32_t axis = 0;
+    bool leaf = false;
+};
+
+struct BuiltScene {
+    // Geometry in world space, reference TriAccel numbering.
+    int64_t num_tris = 0;
+    std::vector<float> positions;     // 3 per world vertex
+    std::vector<float> normals;       // 3 per world vertex
+    std::vector<float> texcoords;     // 2 per world vertex (zeros when absent)
+    std::vector<uint32_t> tri_vidx;   // 3 per triangle, into the world vertex arrays
+    std::vector<int32_t> tri_prim;    // primitive of each triangle
+    std::vector<uint8_t> has_uv;      // per primitive
+    HostAabb bounds;                  // GetAABBTriangles()
+
+    // Reference-exact BVH.
+    std::vector<BuildNode> nodes;     // arbitrary order
+    int32_t root = -1;
+    std::vector<int32_t> tri_order;   // bvhTriIndices
+    int64_t num_leaves = 0;
+    int32_t max_depth = 0;
+
+    // Device layouts.
+    std::vector<TriRecord> tris;      // leaf order
+    std::vector<Bvh2Node> bvh2;
+    int32_t bvh2_root = 0;            // root reference
+    float root_box[6] = {0, 0, 0, 0, 0, 0};
+    std::vector<Bvh4Node> bvh4;
+    int32_t bvh4_root = 0;
+    int32_t max_stack = 0;            // traversal stack bound for this tree
+    double build_seconds = 0.0;
+};
+
+struct PrimitiveInput {
+    const float* positions;
+    const float* normals;
+    const float* texcoords;
+    const uint32_t* faces;
+    int32_t num_vertices;
+    int32_t num_faces;
+    const float* transform;   // 16 floats column-major or nullptr
+};
+
+// Builds everything; returns an empty string on success, else an error.
+std::string build_scene(const std::vector<PrimitiveInput>& prims, int threads, bool want_bvh,
+                        BuiltScene& out);
+
+}  // namespace lmgpu

@@ -1,0 +1,50 @@
+// Host-side internals shared by the CUDA translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+#include <vector>
+#include "../../include/lmgpu.h"
+#include "scene.cuh"
+
+// Staging for the host-buffer entry points: two streams, each with a device
+// chunk of AoS rays and SoA hits.
+struct HostPipeline {
+    bool ready = false;
+    int64_t chunk = 0;
+    cudaStream_t stream[2] = { nullptr, nullptr };
+    float* rays[2] = { nullptr, nullptr };
+    float* hits[2] = { nullptr, nullptr };
+};
+
+struct LmgpuScene {
+    lmgpu::DeviceScene dev{};
+    LmgpuSceneInfo info{};
+    std::vector<void*> allocations;   // device buffers owned by the scene
+    int device = 0;
+    int32_t* d_status = nullptr;      // device error word (0 = ok)
+    HostPipeline pipe;
+    // Host copies needed by host-side helpers (light selection tables etc.)
+    std::vector<float> bounds_min, bounds_max;
+};
+
+namespace lmgpu {
+
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+// Device error word values (OR-ed together by kernels).
+constexpr int32_t STATUS_STACK_OVERFLOW = 1;
+constexpr int32_t STATUS_QUEUE_OVERFLOW = 2;
+constexpr int32_t STATUS_TIMEOUT = 4;
+
+// Reads and clears the device status word; maps it to an LMGPU status.
+int consume_status(LmgpuScene* s, cudaStream_t stream);
+
+}  // namespace lmgpu
+
+#define LMGPU_CUDA_TRY(expr)                                              \
+    do {                                                                  \
+        cudaError_t e_ = (expr);                                          \
+        if (e_ != cudaSuccess) return lmgpu::cuda_fail(e_, #expr);        \
+    } while (0)

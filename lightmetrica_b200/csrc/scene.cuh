@@ -1,0 +1,70 @@
+// Device view of a built scene (all pointers are device memory), shared by
+// the intersection and path-tracing kernels.
+#pragma once
+#include <cstdint>
+#include "layout.h"
+
+namespace lmgpu {
+
+struct AreaLightGpu {
+    float Le[3];
+    float area, inv_area;
+    int32_t cdf_begin;     // into DeviceScene::light_cdf / light_tris
+    int32_t num_tris;
+    int32_t pad;
+};
+
+// Pinhole camera (reference perspectivecamera.cpp:97-353). Matrices are
+// column-major 4x4 like Math::Mat4.
+struct CameraGpu {
+    float view[16];
+    float inv_view[16];
+    float proj[16];
+    float inv_proj[16];
+    float position[3];
+    float inv_A;           // 1 / sensor area at distance 1
+    int32_t width, height;
+    int32_t valid;
+    int32_t pad;
+};
+
+struct DeviceScene {
+    // ---- accelerator
+    int32_t layout;
+    int32_t root_ref;      // BVH2 root reference
+    int32_t root_ref4;     // BVH4 root reference
+    int32_t stack_cap;
+    float root_box[6];     // lo.xyz, hi.xyz
+    const Bvh2Node* bvh2;
+    const Bvh4Node* bvh4;
+    const TriRecord* tris;        // leaf order
+    const TriRecord* tris_by_id;  // TriAccel order (naive layout)
+    int64_t num_tris;
+
+    // ---- geometry, TriAccel numbering
+    const float* vpos;            // 3 per world vertex
+    const float* vnrm;
+    const float* vuv;
+    const uint32_t* tri_vidx;     // 3 per triangle
+    const int32_t* tri_prim;
+    const int32_t* prim_material; // per primitive
+    const int32_t* prim_light;    // per primitive: area light index or -1
+    const float4* materials;      // (R.xyz, type bits)
+    int32_t num_materials;
+
+    // ---- lights: area lights [0, num_area_lights), then the environment
+    int32_t num_area_lights;
+    int32_t num_lights;
+    int32_t has_env;
+    const AreaLightGpu* area_lights;
+    const float* light_cdf;       // per light: num_tris + 1 entries
+    const int32_t* light_tris;    // triangle ids per light
+    float env_Le[3];
+    float env_center[3];
+    float env_radius;
+    float env_inv_area;
+
+    CameraGpu cam;
+};
+
+}  // namespace lmgpu

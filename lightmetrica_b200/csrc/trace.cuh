@@ -1,0 +1,224 @@
+// Device-side ray traversal for sm_100a.
+//
+// Exactness contract: for LMGPU_LAYOUT_BVH2 the closest hit (triangle id, t,
+// u, v) is bit-identical to the reference BVHScene::Intersect
+// (scene.bvh.cpp:405-473, TriAccel::Intersect triaccel.h:100-160):
+//   * same tree (host builder) and the same near-first depth-first order
+//     (the right child first iff the ray direction is negative along the
+//     node's split axis);
+//   * the slab test's maxT-independent part is evaluated when a node is
+//     first seen; its `tmin < maxT` part is re-evaluated when the far child is
+//     popped, i.e. with the same maxT the recursive reference sees there;
+//   * every float operation uses an explicit round-to-nearest intrinsic
+//     (__fadd_rn, __fmul_rn, __fdiv_rn, ...), so nvcc cannot fuse them into
+//     FMAs and each rounds once, like the reference's float SSE build.
+#pragma once
+#include <cfloat>
+#include <cstdint>
+#include "layout.h"
+
+namespace lmgpu {
+
+struct RayIn {
+    float o[3], d[3];
+    float tmin, tmax;
+};
+
+struct TraversalRay {
+    float o[3];
+    float d[3];
+    float inv_min[3];   // 1/d, or 0 where d == 0      (scene.bvh.cpp:124-127)
+    float inv_max[3];   // 1/d, or FLT_MAX where d == 0 (scene.bvh.cpp:129-132)
+    uint32_t neg;       // bit c set iff d[c] < 0        (scene.bvh.cpp:134-137)
+    float tmin, tmax;
+};
+
+__device__ __forceinline__ void setup_ray(TraversalRay& r, const RayIn& in)
+{
+    r.neg = 0;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        r.o[c] = in.o[c];
+        r.d[c] = in.d[c];
+        const bool z = in.d[c] == 0.0f;
+        const float inv = __frcp_rn(in.d[c]);  // correctly rounded 1/d == 1.0f/d
+        r.inv_min[c] = z ? 0.0f : inv;
+        r.inv_max[c] = z ? FLT_MAX : inv;
+        r.neg |= (in.d[c] < 0.0f ? 1u : 0u) << c;
+    }
+    r.tmin = in.tmin;
+    r.tmax = in.tmax;
+}
+
+// Slab test of one box, split into the maxT-independent verdict (`pass`)
+// and the entry distance `t_enter`; the box is hit iff pass && t_enter < maxT.
+// lo/hi are the box's per-axis bounds.
+__device__ __forceinline__ bool slab_intrinsic(const TraversalRay& r,
+                                               float lox, float hix, float loy, float hiy,
+                                               float loz, float hiz, float& t_enter)
+{
+    const float nx = (r.neg & 1u) ? hix : lox, fx = (r.neg & 1u) ? lox : hix;
+    const float ny = (r.neg & 2u) ? hiy : loy, fy = (r.neg & 2u) ? loy : hiy;
+    const float nz = (r.neg & 4u) ? hiz : loz, fz = (r.neg & 4u) ? loz : hiz;
+    float tmin = __fmul_rn(__fsub_rn(nx, r.o[0]), r.inv_min[0]);
+    float tmax = __fmul_rn(__fsub_rn(fx, r.o[0]), r.inv_max[0]);
+    const float tymin = __fmul_rn(__fsub_rn(ny, r.o[1]), r.inv_min[1]);
+    const float tymax = __fmul_rn(__fsub_rn(fy, r.o[1]), r.inv_max[1]);
+    if ((tmin > tymax) || (tymin > tmax)) return false;
+    if (tymin > tmin) tmin = tymin;
+    if (tymax < tmax) tmax = tymax;
+    const float tzmin = __fmul_rn(__fsub_rn(nz, r.o[2]), r.inv_min[2]);
+    const float tzmax = __fmul_rn(__fsub_rn(fz, r.o[2]), r.inv_max[2]);
+    if ((tmin > tzmax) || (tzmin > tmax)) return false;
+    if (tzmin > tmin) tmin = tzmin;
+    if (tzmax < tmax) tmax = tzmax;
+    t_enter = tmin;
+    return tmax > r.tmin;
+}
+
+// TriAccel::Intersect (triaccel.h:100-160) in the reference's order.
+// Returns true on a hit within [mint, maxt]; u, v, t are then valid.
+__device__ __forceinline__ bool triaccel_intersect(const float4 q0, const float4 q1, const float4 q2,
+                                                   const TraversalRay& r, float maxt,
+                                                   float& u, float& v, float& t)
+{
+    const uint32_t k = __float_as_uint(q0.x) & TRI_AXIS_MASK;
+    if (k == 3u) return false;
+    // (u, v, k) axis permutation: k=0 -> (1,2,0), k=1 -> (2,0,1), k=2 -> (0,1,2)
+    const float o_u = k == 0 ? r.o[1] : (k == 1 ? r.o[2] : r.o[0]);
+    const float o_v = k == 0 ? r.o[2] : (k == 1 ? r.o[0] : r.o[1]);
+    const float o_k = k == 0 ? r.o[0] : (k == 1 ? r.o[1] : r.o[2]);
+    const float d_u = k == 0 ? r.d[1] : (k == 1 ? r.d[2] : r.d[0]);
+    const float d_v = k == 0 ? r.d[2] : (k == 1 ? r.d[0] : r.d[1]);
+    const float d_k = k == 0 ? r.d[0] : (k == 1 ? r.d[1] : r.d[2]);
+    const float n_u = q0.y, n_v = q0.z, n_d = q0.w;
+    const float a_u = q1.x, a_v = q1.y, b_nu = q1.z, b_nv = q1.w;
+    const float c_nu = q2.x, c_nv = q2.y;
+    float num = __fsub_rn(n_d, __fmul_rn(o_u, n_u));
+    num = __fsub_rn(num, __fmul_rn(o_v, n_v));
+    num = __fsub_rn(num, o_k);
+    float den = __fadd_rn(__fmul_rn(d_u, n_u), __fmul_rn(d_v, n_v));
+    den = __fadd_rn(den, d_k);
+    t = __fdiv_rn(num, den);
+    if (t < r.tmin || t > maxt) return false;
+    const float hu = __fsub_rn(__fadd_rn(o_u, __fmul_rn(t, d_u)), a_u);
+    const float hv = __fsub_rn(__fadd_rn(o_v, __fmul_rn(t, d_v)), a_v);
+    u = __fadd_rn(__fmul_rn(hv, b_nu), __fmul_rn(hu, b_nv));
+    v = __fadd_rn(__fmul_rn(hu, c_nu), __fmul_rn(hv, c_nv));
+    return u >= 0.0f && v >= 0.0f && __fadd_rn(u, v) <= 1.0f;
+}
+
+struct Hit {
+    int32_t tri;   // reference TriAccel index, -1 = miss
+    float t, u, v;
+};
+
+struct TraceStats {
+    uint32_t nodes;   // binary-node slab tests (reference count)
+    uint32_t tris;    // TriAccel tests
+};
+
+// Leaf loop: every record of the leaf is tested against the running maxT;
+// a hit sets maxT = t so later records need t <= new maxT (scene.bvh.cpp:416-427).
+template <bool ANY_HIT>
+__device__ __forceinline__ bool trace_leaf(const TriRecord* __restrict__ tris, int32_t first,
+                                           TraversalRay& r, Hit& h, TraceStats* st)
+{
+    const float4* p = reinterpret_cast<const float4*>(tris + first);
+    for (;;) {
+        const float4 q0 = __ldg(p), q1 = __ldg(p + 1), q2 = __ldg(p + 2);
+        if (st) st->tris++;
+        float u, v, t;
+        if (triaccel_intersect(q0, q1, q2, r, r.tmax, u, v, t)) {
+            r.tmax = t;
+            h.tri = static_cast<int32_t>(__float_as_uint(q2.z));
+            h.t = t; h.u = u; h.v = v;
+            if (ANY_HIT) return true;
+        }
+        if (__float_as_uint(q0.x) & TRI_LAST_IN_LEAF) break;
+        p += 3;
+    }
+    return false;
+}
+
+// Closest hit (or any hit) through the binary children-in-parent BVH.
+// `stack` is per-thread scratch of `stack_cap` (ref, t_enter) pairs.
+// Returns false if the stack bound was exceeded (the caller flags an error).
+template <bool ANY_HIT>
+__device__ __forceinline__ bool trace_bvh2(const Bvh2Node* __restrict__ nodes,
+                                           const TriRecord* __restrict__ tris,
+                                           int32_t root_ref, const float* root_box,
+                                           TraversalRay& r, Hit& h, int2* stack, int stack_cap,
+                                           TraceStats* st)
+{
+    h.tri = -1;
+    // Root box test (the reference tests every node's own box on entry).
+    float te;
+    if (st) st->nodes++;
+    if (!slab_intrinsic(r, root_box[0], root_box[3], root_box[1], root_box[4], root_box[2], root_box[5], te) ||
+        !(te < r.tmax))
+        return true;
+    int sp = 0;
+    int32_t ref = root_ref;
+    for (;;) {
+        if (ref >= 0) {
+            const float4* np = reinterpret_cast<const float4*>(nodes + ref);
+            const float4 bx = __ldg(np), by = __ldg(np + 1), bz = __ldg(np + 2);
+            const int4 meta = __ldg(reinterpret_cast<const int4*>(np + 3));
+            float tl = 0.f, tr = 0.f;
+            const bool pl = slab_intrinsic(r, bx.x, bx.y, by.x, by.y, bz.x, bz.y, tl);
+            const bool pr = slab_intrinsic(r, bx.z, bx.w, by.z, by.w, bz.z, bz.w, tr);
+            const bool right_first = (r.neg >> meta.z) & 1u;
+            const int32_t near_ref = right_first ? meta.y : meta.x;
+            const int32_t far_ref = right_first ? meta.x : meta.y;
+            const bool near_pass = right_first ? pr : pl;
+            const bool far_pass = right_first ? pl : pr;
+            const float near_t = right_first ? tr : tl;
+            const float far_t = right_first ? tl : tr;
+            if (st) st->nodes++;                         // near child's slab test
+            if (near_pass && near_t < r.tmax) {
+                if (far_pass) {
+                    if (sp >= stack_cap) return false;
+                    stack[sp++] = make_int2(far_ref, __float_as_int(far_t));
+                } else if (st) {
+                    st->nodes++;                         // far child's (failing) test
+                }
+                ref = near_ref;
+                continue;
+            }
+            if (st) st->nodes++;                         // far child's test, same maxT
+            if (far_pass && far_t < r.tmax) { ref = far_ref; continue; }
+        } else {
+            if (trace_leaf<ANY_HIT>(tris, ~ref, r, h, st) && ANY_HIT) return true;
+        }
+        // Pop the next far child whose box is still entered before maxT.
+        for (;;) {
+            if (sp == 0) return true;
+            const int2 e = stack[--sp];
+            if (st) st->nodes++;                         // deferred far-child test
+            if (__int_as_float(e.y) < r.tmax) { ref = e.x; break; }
+        }
+    }
+}
+
+// Brute force over all records in TriAccel order (reference scene.naive.cpp:98-121).
+template <bool ANY_HIT>
+__device__ __forceinline__ void trace_naive(const TriRecord* __restrict__ tris_in_id_order, int64_t n,
+                                            TraversalRay& r, Hit& h, TraceStats* st)
+{
+    h.tri = -1;
+    const float4* p = reinterpret_cast<const float4*>(tris_in_id_order);
+    for (int64_t i = 0; i < n; i++, p += 3) {
+        const float4 q0 = __ldg(p), q1 = __ldg(p + 1), q2 = __ldg(p + 2);
+        if (st) st->tris++;
+        float u, v, t;
+        if (triaccel_intersect(q0, q1, q2, r, r.tmax, u, v, t)) {
+            r.tmax = t;
+            h.tri = static_cast<int32_t>(__float_as_uint(q2.z));
+            h.t = t; h.u = u; h.v = v;
+            if (ANY_HIT) return;
+        }
+    }
+}
+
+}  // namespace lmgpu

@@ -1,0 +1,109 @@
+"""Renderer / RenderProcessScheduler side of the component mirror
+(reference renderer.h:39-133, sched.h:52-127, pathtrace.cpp:122-154,
+sched.mt.cpp:41-266).
+
+The reference's schedulers call ProcessSingleSample once per sample; on the
+GPU the scheduler hands the whole `num_samples` budget to one C-ABI call and
+writes the film with the reference's rescale semantics
+(Rescale(W * H / num_samples), sched.mt.cpp:250-256).
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+
+from . import native as N
+
+_TECHNIQUES = {"pt": N.RENDER_PT, "pt.direct": N.RENDER_PT_DIRECT, "pt.mis": N.RENDER_PT_MIS,
+               "plugin.gpupt": N.RENDER_PT}
+
+
+class Renderer:
+    """Reference Renderer component ("pt", "pt.direct", "pt.mis")."""
+
+    def __init__(self, impl: str = "pt"):
+        if impl not in _TECHNIQUES:
+            raise ValueError(f"unknown renderer '{impl}'")
+        self.impl = impl
+        self.technique = _TECHNIQUES[impl]
+        self.rr_depth = 1
+        self.max_path_vertices = -1
+        self.seed = 1
+        self.sampling = N.SAMPLING_STRATIFIED
+
+    def type(self) -> str:
+        return self.impl
+
+    def configure(self, node: Optional[dict] = None, assets=None, scene=None, sched=None) -> bool:
+        """Reads `rr_depth` (default 1), `max_path_vertices` (default -1) and
+        `sampler` {`rng_seed`, `sampling`} like pathtrace.cpp:122-154."""
+        node = node or {}
+        self.rr_depth = int(node.get("rr_depth", 1))
+        self.max_path_vertices = int(node.get("max_path_vertices", -1))
+        sampler = node.get("sampler", {}) or {}
+        self.seed = int(sampler.get("rng_seed", 1))
+        mode = sampler.get("sampling", "stratified")
+        if mode not in ("stratified", "uniform"):
+            raise ValueError("sampler.sampling must be 'stratified' or 'uniform'")
+        self.sampling = N.SAMPLING_STRATIFIED if mode == "stratified" else N.SAMPLING_UNIFORM
+        return True
+
+    def params(self, num_samples: int, sample_offset: int = 0, film_fp64: bool = False, wave_paths: int = 0):
+        p = N.RenderParams()
+        p.technique = self.technique
+        p.rr_depth = self.rr_depth
+        p.max_path_vertices = self.max_path_vertices
+        p.sampling = self.sampling
+        p.seed = self.seed
+        p.num_samples = int(num_samples)
+        p.sample_offset = int(sample_offset)
+        p.film_fp64 = 1 if film_fp64 else 0
+        p.wave_paths = int(wave_paths)
+        return p
+
+
+class RenderProcessScheduler:
+    """Reference scheduler ("mt"): renders the whole sample budget. On the GPU
+    this is one batched call; `num_threads`/`samples_per_block` are accepted
+    for configuration compatibility and ignored."""
+
+    def __init__(self, impl: str = "mt"):
+        self.impl = impl
+        self.num_samples = 1
+        self.film_fp64 = False
+        self.wave_paths = 0
+        self.last_stats = None
+
+    def configure(self, node: Optional[dict] = None, assets=None) -> bool:
+        node = node or {}
+        self.num_samples = int(node.get("num_samples", 1))
+        self.film_fp64 = bool(node.get("film_fp64", False))
+        self.wave_paths = int(node.get("wave_paths", 0))
+        if self.num_samples <= 0:
+            raise ValueError("num_samples must be positive")
+        return True
+
+    def render(self, renderer: Renderer, scene) -> np.ndarray:
+        """RenderProcessScheduler::Render: returns the rescaled film (H, W, 3)
+        and stores it in the main camera's film."""
+        cam = scene.main_camera()
+        if cam is None or cam.film is None:
+            raise RuntimeError("scene has no main camera / film")
+        film = np.zeros((cam.film.height, cam.film.width, 3), np.float32)
+        p = renderer.params(self.num_samples, film_fp64=self.film_fp64, wave_paths=self.wave_paths)
+        st = N.RenderStats()
+        N.check(N.lib().lmgpu_render(scene.handle, ctypes.byref(p), film.ctypes.data, ctypes.byref(st)))
+        self.last_stats = {"rays_traced": st.rays_traced, "shadow_rays": st.shadow_rays, "paths": st.paths,
+                           "waves": st.waves, "max_bounces_run": st.max_bounces_run, "device_ms": st.device_ms}
+        cam.film.data = film
+        return film
+
+
+def create_renderer(impl: str = "pt") -> Renderer:
+    return Renderer(impl)
+
+
+def create_scheduler(impl: str = "mt") -> RenderProcessScheduler:
+    return RenderProcessScheduler(impl)

@@ -14,6 +14,8 @@ Fixtures:
                            benchmark's distributions (4096 tris, edge sigma
                            0.16, 8192 rays);
                            reference BVHScene tri ids, t and (u, v)
+  soup_duplicates.npz      1024 triangles, each repeated three times (exact
+                           ties), 4096 rays; reference bvh and naive ids and t
 Each fixture stores the inputs with the reference outputs for every scene
 type the reference builds here (bvh, qbvh, naive).
 """
@@ -105,6 +107,24 @@ def main():
     np.savez_compressed(os.path.join(OUT, "soup_small.npz"), positions=pos, faces=faces, rays=rays4,
                         bvh_tri_id=r["tri_id"], bvh_t=r["t"], bvh_u=r["uv"][:, 0], bvh_v=r["uv"][:, 1])
     print("wrote soup_small.npz hits", int((r["tri_id"] >= 0).sum()))
+
+    # Exact ties: every triangle appears three times. The reference keeps the
+    # last of equal-t hits in leaf order (t <= maxT is accepted,
+    # scene.bvh.cpp:416-427), so the returned id pins the partition order
+    # (std::partition, scene.bvh.cpp:375) and the naive scan order.
+    base, _ = random_soup(1024, seed=13, sigma=0.16)
+    tri = base.reshape(-1, 3, 3)
+    dup = np.repeat(tri, 3, axis=0).reshape(-1, 3).astype(np.float32)
+    fd = np.arange(dup.shape[0], dtype=np.uint32).reshape(-1, 3)
+    rays5 = random_rays(4096, seed=14)
+    out = dict(positions=dup, faces=fd, rays=rays5)
+    for typ in ("bvh", "naive"):
+        s = oracle.RefScene(dup, fd, typ)
+        r = s.intersect(rays5, geom=True)
+        out[f"{typ}_tri_id"] = r["tri_id"]
+        out[f"{typ}_t"] = r["t"]
+    np.savez_compressed(os.path.join(OUT, "soup_duplicates.npz"), **out)
+    print("wrote soup_duplicates.npz hits", int((out["bvh_tri_id"] >= 0).sum()))
 
 
 if __name__ == "__main__":
