@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--layout", default="bvh", choices=["bvh", "qbvh"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
+    ap.add_argument("--rays-log2", type=int, default=24, help="ray batch 2^k (profiling runs use less)")
     return ap.parse_args()
 
 
@@ -203,9 +204,9 @@ def run_reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
-def workload_config(layout):
-    return {"workload": "ray-intersection: 2^24 rays x 1,048,576-triangle soup, closest hit",
-            "rays": NUM_RAYS, "triangles": NUM_TRIS,
+def workload_config(layout, rays=NUM_RAYS):
+    return {"workload": f"ray-intersection: 2^{rays.bit_length() - 1} rays x 1,048,576-triangle soup, closest hit",
+            "rays": rays, "triangles": NUM_TRIS,
             "layout": {"bvh": "binary SAH BVH (reference bvh, bit-exact)",
                        "qbvh": "4-wide collapse of the reference tree (bit-exact)"}[layout],
             "l2": "inputs larger than L2 (512 MB of rays per step); no flush"}
@@ -227,14 +228,15 @@ def run_ours(args):
     from lightmetrica_b200.workloads import random_rays, random_soup, rays_soa
 
     pos, faces = random_soup(NUM_TRIS, seed=1)
-    rays = random_rays(NUM_RAYS, seed=2 + rank)
+    num_rays = 1 << args.rays_log2
+    rays = random_rays(num_rays, seed=2 + rank)
     scene = Scene(args.layout)
     scene.load(soup_primitives(pos, faces))
     scene.configure({})
     scene.build()
     info = scene.info()
 
-    n = NUM_RAYS
+    n = num_rays
     soa = {k: torch.from_numpy(v).to(dev) for k, v in rays_soa(rays).items()}
     hits = {"tri_id": torch.empty(n, dtype=torch.int32, device=dev)}
     for k in ("t", "u", "v"):
@@ -310,7 +312,7 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded; no public scene exists for this workload)",
-            "config": dict(workload_config(args.layout), parallelism=f"replicas x{world}",
+            "config": dict(workload_config(args.layout, n), parallelism=f"replicas x{world}",
                            hit_fraction=round(hit_frac, 4), bvh_nodes=info["num_nodes"], bvh_depth=info["max_depth"],
                            build_seconds=round(info["build_seconds"], 3)),
             "e2e": e2e,

@@ -12,6 +12,9 @@
 #include "internal.h"
 #include "trace.cuh"
 #include "trace4.cuh"
+#include "trace_kernels.cuh"
+#include <mutex>
+#include <unordered_map>
 
 namespace lmgpu {
 
@@ -42,6 +45,22 @@ int consume_status(LmgpuScene* s, cudaStream_t stream)
     if (st & STATUS_QUEUE_OVERFLOW) return fail(LMGPU_ERR_QUEUE_OVERFLOW, "wavefront queue bound exceeded");
     if (st & STATUS_TIMEOUT) return fail(LMGPU_ERR_TIMEOUT, "bounded device wait gave up");
     return fail(LMGPU_ERR_CUDA, "unknown device status");
+}
+
+int resident_blocks_of(const void* kernel)
+{
+    static std::mutex mu;
+    static std::unordered_map<const void*, int> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(kernel);
+    if (it != cache.end()) return it->second;
+    int per_sm = 0, sms = 0, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, 0);
+    const int b = std::max(1, per_sm) * std::max(1, sms);
+    cache[kernel] = b;
+    return b;
 }
 
 namespace {
@@ -278,12 +297,15 @@ int create_impl(const LmgpuSceneDesc* desc, LmgpuScene** out)
     }
     if (rc != LMGPU_OK) { lmgpu_scene_destroy(s); return rc; }
 
+    // Scratch: status word and the persistent kernels' work counter.
     void* st = nullptr;
-    cudaError_t e = cudaMalloc(&st, sizeof(int32_t));
+    const size_t scratch = 256 + LmgpuScene::WORK_SLOTS * sizeof(unsigned long long);
+    cudaError_t e = cudaMalloc(&st, scratch);
     if (e != cudaSuccess) { lmgpu_scene_destroy(s); return cuda_fail(e, "cudaMalloc(status)"); }
     s->allocations.push_back(st);
     s->d_status = static_cast<int32_t*>(st);
-    LMGPU_CUDA_TRY(cudaMemset(s->d_status, 0, sizeof(int32_t)));
+    s->d_work = reinterpret_cast<unsigned long long*>(static_cast<char*>(st) + 256);
+    LMGPU_CUDA_TRY(cudaMemset(st, 0, scratch));
 
     LmgpuSceneInfo& info = s->info;
     info.num_triangles = b.num_tris;
@@ -313,16 +335,17 @@ struct RaySrc {
 __device__ __forceinline__ RayIn load_ray(const RaySrc& R, int64_t i)
 {
     RayIn in;
+    // Rays are read once: streaming loads keep them from evicting the BVH in L2.
     if (R.aos) {
-        const float4 a = __ldg(R.aos + 2 * i), b = __ldg(R.aos + 2 * i + 1);
+        const float4 a = __ldcs(R.aos + 2 * i), b = __ldcs(R.aos + 2 * i + 1);
         in.o[0] = a.x; in.o[1] = a.y; in.o[2] = a.z;
         in.d[0] = a.w; in.d[1] = b.x; in.d[2] = b.y;
         in.tmin = b.z; in.tmax = b.w;
         return in;
     }
-    in.o[0] = __ldg(R.soa.ox + i); in.o[1] = __ldg(R.soa.oy + i); in.o[2] = __ldg(R.soa.oz + i);
-    in.d[0] = __ldg(R.soa.dx + i); in.d[1] = __ldg(R.soa.dy + i); in.d[2] = __ldg(R.soa.dz + i);
-    in.tmin = __ldg(R.soa.tmin + i); in.tmax = __ldg(R.soa.tmax + i);
+    in.o[0] = __ldcs(R.soa.ox + i); in.o[1] = __ldcs(R.soa.oy + i); in.o[2] = __ldcs(R.soa.oz + i);
+    in.d[0] = __ldcs(R.soa.dx + i); in.d[1] = __ldcs(R.soa.dy + i); in.d[2] = __ldcs(R.soa.dz + i);
+    in.tmin = __ldcs(R.soa.tmin + i); in.tmax = __ldcs(R.soa.tmax + i);
     return in;
 }
 
@@ -368,40 +391,46 @@ __global__ void __launch_bounds__(128) k_intersect(const DeviceScene s, const Ra
     }
 }
 
-template <int LAYOUT, int STACK>
-__global__ void __launch_bounds__(128) k_occluded(const DeviceScene s, const RaySrc rays, int64_t n,
-                                                  uint8_t* occluded, int32_t* status)
+__device__ __forceinline__ void store_hit(const LmgpuHitsSoA& hits, int64_t i, const Hit& h)
 {
-    int2 stack[STACK];
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    TraversalRay r;
-    setup_ray(r, load_ray(rays, i));
-    Hit h;
-    const bool ok = trace_one<LAYOUT, true, STACK>(s, r, h, stack, nullptr);
-    if (!ok) atomicOr(status, STATUS_STACK_OVERFLOW);
-    occluded[i] = h.tri >= 0 ? 1 : 0;
+    const bool hit = h.tri >= 0;
+    if (hits.tri_id) __stcs(hits.tri_id + i, h.tri);
+    if (hits.t) __stcs(hits.t + i, hit ? h.t : 0.0f);
+    if (hits.u) __stcs(hits.u + i, hit ? h.u : 0.0f);
+    if (hits.v) __stcs(hits.v + i, hit ? h.v : 0.0f);
 }
 
+// I/O policy of the intersection API: SoA or AoS rays in, hit arrays out.
+struct ApiHitIO {
+    RaySrc rays;
+    int64_t n;
+    LmgpuHitsSoA hits;
+    __device__ int64_t count() const { return n; }
+    __device__ RayIn load(int64_t i) const { return load_ray(rays, i); }
+    __device__ void store(int64_t i, const Hit& h, const TraversalRay&) const { store_hit(hits, i, h); }
+};
+
+// I/O policy of the visibility API: occluded flag per ray.
+struct ApiAnyIO {
+    RaySrc rays;
+    int64_t n;
+    uint8_t* occluded;
+    __device__ int64_t count() const { return n; }
+    __device__ RayIn load(int64_t i) const { return load_ray(rays, i); }
+    __device__ void store(int64_t i, const Hit& h, const TraversalRay&) const { occluded[i] = h.tri >= 0 ? 1 : 0; }
+};
+
 template <int STACK>
-int launch_intersect_stack(LmgpuScene* sc, const RaySrc& rays, int64_t n, const LmgpuHitsSoA& hits,
-                           cudaStream_t stream, unsigned long long* counters)
+int launch_counted_stack(LmgpuScene* sc, const RaySrc& rays, int64_t n, const LmgpuHitsSoA& hits,
+                         cudaStream_t stream, unsigned long long* counters)
 {
     const int threads = 128;
     const int64_t blocks = (n + threads - 1) / threads;
     const DeviceScene& s = sc->dev;
-    if (counters) {
-        switch (s.layout) {
-        case LMGPU_LAYOUT_BVH2: k_intersect<LMGPU_LAYOUT_BVH2, STACK, true><<<blocks, threads, 0, stream>>>(s, rays, n, hits, sc->d_status, counters); break;
-        case LMGPU_LAYOUT_BVH4: k_intersect<LMGPU_LAYOUT_BVH4, STACK, true><<<blocks, threads, 0, stream>>>(s, rays, n, hits, sc->d_status, counters); break;
-        default: k_intersect<LMGPU_LAYOUT_NAIVE, 1, true><<<blocks, threads, 0, stream>>>(s, rays, n, hits, sc->d_status, counters); break;
-        }
-    } else {
-        switch (s.layout) {
-        case LMGPU_LAYOUT_BVH2: k_intersect<LMGPU_LAYOUT_BVH2, STACK, false><<<blocks, threads, 0, stream>>>(s, rays, n, hits, sc->d_status, nullptr); break;
-        case LMGPU_LAYOUT_BVH4: k_intersect<LMGPU_LAYOUT_BVH4, STACK, false><<<blocks, threads, 0, stream>>>(s, rays, n, hits, sc->d_status, nullptr); break;
-        default: k_intersect<LMGPU_LAYOUT_NAIVE, 1, false><<<blocks, threads, 0, stream>>>(s, rays, n, hits, sc->d_status, nullptr); break;
-        }
+    switch (s.layout) {
+    case LMGPU_LAYOUT_BVH2: k_intersect<LMGPU_LAYOUT_BVH2, STACK, true><<<blocks, threads, 0, stream>>>(s, rays, n, hits, sc->d_status, counters); break;
+    case LMGPU_LAYOUT_BVH4: k_intersect<LMGPU_LAYOUT_BVH4, STACK, true><<<blocks, threads, 0, stream>>>(s, rays, n, hits, sc->d_status, counters); break;
+    default: k_intersect<LMGPU_LAYOUT_NAIVE, 1, true><<<blocks, threads, 0, stream>>>(s, rays, n, hits, sc->d_status, counters); break;
     }
     LMGPU_CUDA_TRY(cudaGetLastError());
     return LMGPU_OK;
@@ -411,32 +440,18 @@ int launch_intersect(LmgpuScene* sc, const RaySrc& rays, int64_t n, const LmgpuH
                      cudaStream_t stream, unsigned long long* counters)
 {
     if (n == 0) return LMGPU_OK;
+    if (!counters) return launch_trace<false>(sc, ApiHitIO{ rays, n, hits }, n, stream);
     const int cap = sc->dev.stack_cap;
-    if (cap <= 32) return launch_intersect_stack<32>(sc, rays, n, hits, stream, counters);
-    if (cap <= 64) return launch_intersect_stack<64>(sc, rays, n, hits, stream, counters);
-    if (cap <= 128) return launch_intersect_stack<128>(sc, rays, n, hits, stream, counters);
-    if (cap <= 256) return launch_intersect_stack<256>(sc, rays, n, hits, stream, counters);
+    if (cap <= 32) return launch_counted_stack<32>(sc, rays, n, hits, stream, counters);
+    if (cap <= 64) return launch_counted_stack<64>(sc, rays, n, hits, stream, counters);
+    if (cap <= 128) return launch_counted_stack<128>(sc, rays, n, hits, stream, counters);
+    if (cap <= 256) return launch_counted_stack<256>(sc, rays, n, hits, stream, counters);
     return fail(LMGPU_ERR_UNSUPPORTED, "BVH deeper than the largest compiled traversal stack (256)");
 }
 
-template <int STACK>
-int launch_occluded_stack(LmgpuScene* sc, const RaySrc& rays, int64_t n, uint8_t* occ, cudaStream_t stream)
-{
-    const int threads = 128;
-    const int64_t blocks = (n + threads - 1) / threads;
-    const DeviceScene& s = sc->dev;
-    switch (s.layout) {
-    case LMGPU_LAYOUT_BVH2: k_occluded<LMGPU_LAYOUT_BVH2, STACK><<<blocks, threads, 0, stream>>>(s, rays, n, occ, sc->d_status); break;
-    case LMGPU_LAYOUT_BVH4: k_occluded<LMGPU_LAYOUT_BVH4, STACK><<<blocks, threads, 0, stream>>>(s, rays, n, occ, sc->d_status); break;
-    default: k_occluded<LMGPU_LAYOUT_NAIVE, 1><<<blocks, threads, 0, stream>>>(s, rays, n, occ, sc->d_status); break;
-    }
-    LMGPU_CUDA_TRY(cudaGetLastError());
-    return LMGPU_OK;
-}
-
+// Exposed for the measurement path (traversal counters).
 }  // namespace
 
-// Exposed for the measurement path (traversal counters).
 int ensure_host_pipeline(LmgpuScene* sc)
 {
     HostPipeline& hp = sc->pipe;
@@ -488,6 +503,7 @@ int lmgpu_scene_destroy(LmgpuScene* scene)
     if (!scene) return LMGPU_OK;
     if (scene->pipe.ready)
         for (int k = 0; k < 2; k++) cudaStreamDestroy(scene->pipe.stream[k]);
+    release_render_workspace(scene);
     for (void* p : scene->allocations) cudaFree(p);
     delete scene;
     return LMGPU_OK;
@@ -512,14 +528,7 @@ int lmgpu_occluded(LmgpuScene* scene, const LmgpuRaysSoA* rays, int64_t n, uint8
 {
     if (!scene || !rays || !occluded || n < 0) return fail(LMGPU_ERR_INVALID, "null argument or negative count");
     if (n == 0) return LMGPU_OK;
-    const int cap = scene->dev.stack_cap;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const RaySrc src = soa_src(*rays);
-    if (cap <= 32) return launch_occluded_stack<32>(scene, src, n, occluded, st);
-    if (cap <= 64) return launch_occluded_stack<64>(scene, src, n, occluded, st);
-    if (cap <= 128) return launch_occluded_stack<128>(scene, src, n, occluded, st);
-    if (cap <= 256) return launch_occluded_stack<256>(scene, src, n, occluded, st);
-    return fail(LMGPU_ERR_UNSUPPORTED, "BVH deeper than the largest compiled traversal stack (256)");
+    return launch_trace<true>(scene, ApiAnyIO{ soa_src(*rays), n, occluded }, n, static_cast<cudaStream_t>(stream));
 }
 
 int lmgpu_intersect_host(LmgpuScene* scene, const float* rays_aos, int64_t n, int32_t* tri_id, float* t, float* u, float* v)

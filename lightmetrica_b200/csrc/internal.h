@@ -1,6 +1,7 @@
 // Host-side internals shared by the CUDA translation units.
 #pragma once
 #include <cuda_runtime.h>
+#include <atomic>
 #include <string>
 #include <vector>
 #include "../../include/lmgpu.h"
@@ -22,7 +23,14 @@ struct LmgpuScene {
     std::vector<void*> allocations;   // device buffers owned by the scene
     int device = 0;
     int32_t* d_status = nullptr;      // device error word (0 = ok)
+    // Ring of ray counters for the persistent traversal kernels: each launch
+    // takes the next slot, so launches in flight on different streams do not
+    // share a counter (WORK_SLOTS bounds the launches in flight per scene).
+    static constexpr int WORK_SLOTS = 256;
+    unsigned long long* d_work = nullptr;
+    std::atomic<uint64_t> work_slot{0};
     HostPipeline pipe;
+    void* render_ws = nullptr;        // path-tracer wave workspace (pathtrace.cu)
     // Host copies needed by host-side helpers (light selection tables etc.)
     std::vector<float> bounds_min, bounds_max;
 };
@@ -37,6 +45,9 @@ int cuda_fail(cudaError_t e, const char* what);
 constexpr int32_t STATUS_STACK_OVERFLOW = 1;
 constexpr int32_t STATUS_QUEUE_OVERFLOW = 2;
 constexpr int32_t STATUS_TIMEOUT = 4;
+
+// Frees the path tracer's cached workspace of a scene.
+void release_render_workspace(LmgpuScene* sc);
 
 // Reads and clears the device status word; maps it to an LMGPU status.
 int consume_status(LmgpuScene* s, cudaStream_t stream);

@@ -141,6 +141,75 @@ __device__ __forceinline__ bool trace_leaf(const TriRecord* __restrict__ tris, i
     return false;
 }
 
+// Resumable traversal state: the current reference (internal node >= 0,
+// leaf < 0, or REF_DONE) and the deferred far children.
+constexpr int32_t REF_DONE = 0x7fffffff;
+
+struct TravState {
+    int32_t ref;
+    int sp;
+};
+
+// Pops the next deferred child whose box is still entered before maxT
+// (the reference's far-child test, evaluated with the current maxT).
+__device__ __forceinline__ void pop_next(TravState& ts, const int2* stack, const TraversalRay& r, TraceStats* st)
+{
+    while (ts.sp > 0) {
+        const int2 e = stack[--ts.sp];
+        if (st) st->nodes++;
+        if (__int_as_float(e.y) < r.tmax) { ts.ref = e.x; return; }
+    }
+    ts.ref = REF_DONE;
+}
+
+// Root box test (the reference tests every node's own box on entry).
+__device__ __forceinline__ void trav_begin(TravState& ts, int32_t root_ref, const float* root_box,
+                                           const TraversalRay& r, TraceStats* st)
+{
+    ts.sp = 0;
+    float te;
+    if (st) st->nodes++;
+    ts.ref = (slab_intrinsic(r, root_box[0], root_box[3], root_box[1], root_box[4], root_box[2], root_box[5], te) &&
+              te < r.tmax) ? root_ref : REF_DONE;
+}
+
+// Binary children-in-parent nodes: descends until the state reaches a leaf
+// or finishes. Returns false on stack overflow.
+__device__ __forceinline__ bool bvh2_descend(const Bvh2Node* __restrict__ nodes, TravState& ts, int2* stack,
+                                             int stack_cap, const TraversalRay& r, TraceStats* st)
+{
+    while (ts.ref >= 0 && ts.ref != REF_DONE) {
+        const float4* np = reinterpret_cast<const float4*>(nodes + ts.ref);
+        const float4 bx = __ldg(np), by = __ldg(np + 1), bz = __ldg(np + 2);
+        const int4 meta = __ldg(reinterpret_cast<const int4*>(np + 3));
+        float tl = 0.f, tr = 0.f;
+        const bool pl = slab_intrinsic(r, bx.x, bx.y, by.x, by.y, bz.x, bz.y, tl);
+        const bool pr = slab_intrinsic(r, bx.z, bx.w, by.z, by.w, bz.z, bz.w, tr);
+        const bool right_first = (r.neg >> meta.z) & 1u;
+        const int32_t near_ref = right_first ? meta.y : meta.x;
+        const int32_t far_ref = right_first ? meta.x : meta.y;
+        const bool near_pass = right_first ? pr : pl;
+        const bool far_pass = right_first ? pl : pr;
+        const float near_t = right_first ? tr : tl;
+        const float far_t = right_first ? tl : tr;
+        if (st) st->nodes++;                         // near child's slab test
+        if (near_pass && near_t < r.tmax) {
+            if (far_pass) {
+                if (ts.sp >= stack_cap) return false;
+                stack[ts.sp++] = make_int2(far_ref, __float_as_int(far_t));
+            } else if (st) {
+                st->nodes++;                         // far child's (failing) test
+            }
+            ts.ref = near_ref;
+            continue;
+        }
+        if (st) st->nodes++;                         // far child's test, same maxT
+        if (far_pass && far_t < r.tmax) { ts.ref = far_ref; continue; }
+        pop_next(ts, stack, r, st);
+    }
+    return true;
+}
+
 // Closest hit (or any hit) through the binary children-in-parent BVH.
 // `stack` is per-thread scratch of `stack_cap` (ref, t_enter) pairs.
 // Returns false if the stack bound was exceeded (the caller flags an error).
@@ -152,52 +221,13 @@ __device__ __forceinline__ bool trace_bvh2(const Bvh2Node* __restrict__ nodes,
                                            TraceStats* st)
 {
     h.tri = -1;
-    // Root box test (the reference tests every node's own box on entry).
-    float te;
-    if (st) st->nodes++;
-    if (!slab_intrinsic(r, root_box[0], root_box[3], root_box[1], root_box[4], root_box[2], root_box[5], te) ||
-        !(te < r.tmax))
-        return true;
-    int sp = 0;
-    int32_t ref = root_ref;
+    TravState ts;
+    trav_begin(ts, root_ref, root_box, r, st);
     for (;;) {
-        if (ref >= 0) {
-            const float4* np = reinterpret_cast<const float4*>(nodes + ref);
-            const float4 bx = __ldg(np), by = __ldg(np + 1), bz = __ldg(np + 2);
-            const int4 meta = __ldg(reinterpret_cast<const int4*>(np + 3));
-            float tl = 0.f, tr = 0.f;
-            const bool pl = slab_intrinsic(r, bx.x, bx.y, by.x, by.y, bz.x, bz.y, tl);
-            const bool pr = slab_intrinsic(r, bx.z, bx.w, by.z, by.w, bz.z, bz.w, tr);
-            const bool right_first = (r.neg >> meta.z) & 1u;
-            const int32_t near_ref = right_first ? meta.y : meta.x;
-            const int32_t far_ref = right_first ? meta.x : meta.y;
-            const bool near_pass = right_first ? pr : pl;
-            const bool far_pass = right_first ? pl : pr;
-            const float near_t = right_first ? tr : tl;
-            const float far_t = right_first ? tl : tr;
-            if (st) st->nodes++;                         // near child's slab test
-            if (near_pass && near_t < r.tmax) {
-                if (far_pass) {
-                    if (sp >= stack_cap) return false;
-                    stack[sp++] = make_int2(far_ref, __float_as_int(far_t));
-                } else if (st) {
-                    st->nodes++;                         // far child's (failing) test
-                }
-                ref = near_ref;
-                continue;
-            }
-            if (st) st->nodes++;                         // far child's test, same maxT
-            if (far_pass && far_t < r.tmax) { ref = far_ref; continue; }
-        } else {
-            if (trace_leaf<ANY_HIT>(tris, ~ref, r, h, st) && ANY_HIT) return true;
-        }
-        // Pop the next far child whose box is still entered before maxT.
-        for (;;) {
-            if (sp == 0) return true;
-            const int2 e = stack[--sp];
-            if (st) st->nodes++;                         // deferred far-child test
-            if (__int_as_float(e.y) < r.tmax) { ref = e.x; break; }
-        }
+        if (!bvh2_descend(nodes, ts, stack, stack_cap, r, st)) return false;
+        if (ts.ref == REF_DONE) return true;
+        if (trace_leaf<ANY_HIT>(tris, ~ts.ref, r, h, st) && ANY_HIT) return true;
+        pop_next(ts, stack, r, st);
     }
 }
 

@@ -13,6 +13,73 @@
 
 namespace lmgpu {
 
+// 4-wide nodes: descends until the state reaches a leaf or finishes.
+// Returns false on stack overflow.
+__device__ __forceinline__ bool bvh4_descend(const Bvh4Node* __restrict__ nodes, TravState& ts, int2* stack,
+                                             int stack_cap, const TraversalRay& r, TraceStats* st)
+{
+    while (ts.ref >= 0 && ts.ref != REF_DONE) {
+        const float4* np = reinterpret_cast<const float4*>(nodes + ts.ref);
+        const float4 lox = __ldg(np + 0), hix = __ldg(np + 1);
+        const float4 loy = __ldg(np + 2), hiy = __ldg(np + 3);
+        const float4 loz = __ldg(np + 4), hiz = __ldg(np + 5);
+        const int4 child = __ldg(reinterpret_cast<const int4*>(np + 6));
+        const int4 axes = __ldg(reinterpret_cast<const int4*>(np + 7));
+        float t0 = 0.f, t1 = 0.f, t2 = 0.f, t3 = 0.f;
+        const bool p0 = slab_intrinsic(r, lox.x, hix.x, loy.x, hiy.x, loz.x, hiz.x, t0);
+        const bool p1 = slab_intrinsic(r, lox.y, hix.y, loy.y, hiy.y, loz.y, hiz.y, t1);
+        const bool p2 = slab_intrinsic(r, lox.z, hix.z, loy.z, hiy.z, loz.z, hiz.z, t2);
+        const bool p3 = slab_intrinsic(r, lox.w, hix.w, loy.w, hiy.w, loz.w, hiz.w, t3);
+        if (st) st->nodes += 4;
+        // Visit order, 4 bits per slot.
+        uint32_t order = 0;
+        int cnt = 0;
+        const int first_pair = (r.neg >> axes.x) & 1u;
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const int p = q == 0 ? first_pair : 1 - first_pair;
+            const int a = p == 0 ? axes.y : axes.z;
+            if (a < 0) {
+                order |= uint32_t(2 * p) << (4 * cnt); cnt++;
+            } else {
+                const bool sw = (r.neg >> a) & 1u;
+                order |= uint32_t(sw ? 2 * p + 1 : 2 * p) << (4 * cnt); cnt++;
+                order |= uint32_t(sw ? 2 * p : 2 * p + 1) << (4 * cnt); cnt++;
+            }
+        }
+        // Passing children in visit order; the first one entered before maxT
+        // is descended now (same maxT as the reference), later ones are
+        // deferred with their entry distance.
+        int32_t refs[4];
+        float ts4[4];
+        int np_ = 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if (j < cnt) {
+                const uint32_t sl = (order >> (4 * j)) & 0xFu;
+                const bool ps = sl == 0 ? p0 : sl == 1 ? p1 : sl == 2 ? p2 : p3;
+                const float tt = sl == 0 ? t0 : sl == 1 ? t1 : sl == 2 ? t2 : t3;
+                const int32_t cr = sl == 0 ? child.x : sl == 1 ? child.y : sl == 2 ? child.z : child.w;
+                if (ps) { refs[np_] = cr; ts4[np_] = tt; np_++; }
+            }
+        }
+        int first = -1;
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if (first < 0 && j < np_ && ts4[j] < r.tmax) first = j;
+        if (first >= 0) {
+            if (ts.sp + (np_ - 1 - first) > stack_cap) return false;
+#pragma unroll
+            for (int j = 3; j >= 0; j--)
+                if (j > first && j < np_) stack[ts.sp++] = make_int2(refs[j], __float_as_int(ts4[j]));
+            ts.ref = refs[first];
+            continue;
+        }
+        pop_next(ts, stack, r, nullptr);
+    }
+    return true;
+}
+
 template <bool ANY_HIT>
 __device__ __forceinline__ bool trace_bvh4(const Bvh4Node* __restrict__ nodes,
                                            const TriRecord* __restrict__ tris,
@@ -21,81 +88,13 @@ __device__ __forceinline__ bool trace_bvh4(const Bvh4Node* __restrict__ nodes,
                                            TraceStats* st)
 {
     h.tri = -1;
-    float te;
-    if (st) st->nodes++;
-    if (!slab_intrinsic(r, root_box[0], root_box[3], root_box[1], root_box[4], root_box[2], root_box[5], te) ||
-        !(te < r.tmax))
-        return true;
-    int sp = 0;
-    int32_t ref = root_ref;
+    TravState ts;
+    trav_begin(ts, root_ref, root_box, r, st);
     for (;;) {
-        if (ref >= 0) {
-            const float4* np = reinterpret_cast<const float4*>(nodes + ref);
-            const float4 lox = __ldg(np + 0), hix = __ldg(np + 1);
-            const float4 loy = __ldg(np + 2), hiy = __ldg(np + 3);
-            const float4 loz = __ldg(np + 4), hiz = __ldg(np + 5);
-            const int4 child = __ldg(reinterpret_cast<const int4*>(np + 6));
-            const int4 axes = __ldg(reinterpret_cast<const int4*>(np + 7));
-            float t0 = 0.f, t1 = 0.f, t2 = 0.f, t3 = 0.f;
-            const bool p0 = slab_intrinsic(r, lox.x, hix.x, loy.x, hiy.x, loz.x, hiz.x, t0);
-            const bool p1 = slab_intrinsic(r, lox.y, hix.y, loy.y, hiy.y, loz.y, hiz.y, t1);
-            const bool p2 = slab_intrinsic(r, lox.z, hix.z, loy.z, hiy.z, loz.z, hiz.z, t2);
-            const bool p3 = slab_intrinsic(r, lox.w, hix.w, loy.w, hiy.w, loz.w, hiz.w, t3);
-            if (st) st->nodes += 4;
-            // Visit order, 4 bits per slot, 0xF = none.
-            uint32_t order = 0xFFFFu;
-            int cnt = 0;
-            const int first_pair = (r.neg >> axes.x) & 1u;
-#pragma unroll
-            for (int q = 0; q < 2; q++) {
-                const int p = q == 0 ? first_pair : 1 - first_pair;
-                const int a = p == 0 ? axes.y : axes.z;
-                if (a < 0) {
-                    order = (order & ~(0xFu << (4 * cnt))) | (uint32_t(2 * p) << (4 * cnt)); cnt++;
-                } else {
-                    const int s0 = ((r.neg >> a) & 1u) ? 2 * p + 1 : 2 * p;
-                    const int s1 = ((r.neg >> a) & 1u) ? 2 * p : 2 * p + 1;
-                    order = (order & ~(0xFu << (4 * cnt))) | (uint32_t(s0) << (4 * cnt)); cnt++;
-                    order = (order & ~(0xFu << (4 * cnt))) | (uint32_t(s1) << (4 * cnt)); cnt++;
-                }
-            }
-            // Passing children in visit order.
-            int32_t refs[4];
-            float ts[4];
-            int np_ = 0;
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                if (j >= cnt) break;
-                const uint32_t s = (order >> (4 * j)) & 0xFu;
-                const bool ps = s == 0 ? p0 : s == 1 ? p1 : s == 2 ? p2 : p3;
-                const float tt = s == 0 ? t0 : s == 1 ? t1 : s == 2 ? t2 : t3;
-                const int32_t cr = s == 0 ? child.x : s == 1 ? child.y : s == 2 ? child.z : child.w;
-                if (ps) { refs[np_] = cr; ts[np_] = tt; np_++; }
-            }
-            // The first passing child is checked now (same maxT as the
-            // reference); the rest are deferred to the stack.
-            int first = -1;
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                if (j >= np_) break;
-                if (ts[j] < r.tmax) { first = j; break; }
-            }
-            if (first >= 0) {
-                if (sp + (np_ - 1 - first) > stack_cap) return false;
-#pragma unroll
-                for (int j = 3; j >= 0; j--)
-                    if (j > first && j < np_) stack[sp++] = make_int2(refs[j], __float_as_int(ts[j]));
-                ref = refs[first];
-                continue;
-            }
-        } else {
-            if (trace_leaf<ANY_HIT>(tris, ~ref, r, h, st) && ANY_HIT) return true;
-        }
-        for (;;) {
-            if (sp == 0) return true;
-            const int2 e = stack[--sp];
-            if (__int_as_float(e.y) < r.tmax) { ref = e.x; break; }
-        }
+        if (!bvh4_descend(nodes, ts, stack, stack_cap, r, st)) return false;
+        if (ts.ref == REF_DONE) return true;
+        if (trace_leaf<ANY_HIT>(tris, ~ts.ref, r, h, st) && ANY_HIT) return true;
+        pop_next(ts, stack, r, nullptr);
     }
 }
 

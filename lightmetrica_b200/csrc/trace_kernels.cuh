@@ -1,0 +1,147 @@
+// Persistent traversal kernel shared by the intersection API and the path
+// tracer's ray and shadow queues. The I/O policy supplies the ray count, the
+// rays and what to do with each result.
+#pragma once
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <mutex>
+#include <unordered_map>
+#include "internal.h"
+#include "trace.cuh"
+#include "trace4.cuh"
+
+namespace lmgpu {
+
+template <int LAYOUT>
+__device__ __forceinline__ bool descend(const DeviceScene& s, TravState& ts, int2* stack, int cap, const TraversalRay& r)
+{
+    if (LAYOUT == LMGPU_LAYOUT_BVH2) return bvh2_descend(s.bvh2, ts, stack, cap, r, nullptr);
+    return bvh4_descend(s.bvh4, ts, stack, cap, r, nullptr);
+}
+
+// Persistent traversal with per-lane ray replacement: a warp keeps tracing
+// until the batch is exhausted; lanes whose ray has finished take the next
+// rays from a global counter (one warp-aggregated atomic per refill), so short
+// rays do not idle behind long ones. Each ray's walk is the same exact
+// depth-first traversal as trace_bvh2 / trace_bvh4; only the scheduling
+// differs. Lanes alternate "descend to a leaf" and "test the leaf, pop"
+// (while-while) and refill when at least a quarter of the warp is idle.
+template <int LAYOUT, int STACK, bool ANY_HIT, class IO>
+__global__ void __launch_bounds__(128) k_trace_persistent(const DeviceScene s, const IO io, int32_t* status,
+                                                          unsigned long long* next_ray)
+{
+    constexpr unsigned FULL = 0xffffffffu;
+    int2 stack[STACK];
+    const int64_t n = io.count();
+    const unsigned lane = threadIdx.x & 31u;
+    const int32_t root = LAYOUT == LMGPU_LAYOUT_BVH2 ? s.root_ref : s.root_ref4;
+    TraversalRay r;
+    Hit h;
+    h.tri = -1;
+    TravState ts;
+    ts.ref = REF_DONE;
+    ts.sp = 0;
+    int64_t idx = -1;
+    bool exhausted = n <= 0;
+    for (;;) {
+        const bool idle = ts.ref == REF_DONE;
+        const unsigned need = __ballot_sync(FULL, idle);
+        if (!exhausted && (__popc(need) >= 8 || need == FULL)) {
+            const int leader = __ffs(need) - 1;
+            unsigned long long base = 0;
+            if ((int)lane == leader) base = atomicAdd(next_ray, (unsigned long long)__popc(need));
+            base = __shfl_sync(FULL, base, leader);
+            if (base + __popc(need) >= (unsigned long long)n) exhausted = true;
+            if (idle) {
+                idx = (int64_t)base + __popc(need & ((1u << lane) - 1u));
+                if (idx < n) {
+                    setup_ray(r, io.load(idx));
+                    h.tri = -1;
+                    trav_begin(ts, root, s.root_box, r, nullptr);
+                    if (ts.ref == REF_DONE) io.store(idx, h, r);
+                }
+            }
+        } else if (exhausted && need == FULL) {
+            break;
+        }
+        if (ts.ref != REF_DONE) {
+            if (!descend<LAYOUT>(s, ts, stack, STACK, r)) {
+                atomicOr(status, STATUS_STACK_OVERFLOW);
+                h.tri = -1;
+                ts.ref = REF_DONE;
+            } else if (ts.ref != REF_DONE) {
+                if (trace_leaf<ANY_HIT>(s.tris, ~ts.ref, r, h, nullptr) && ANY_HIT) ts.ref = REF_DONE;
+                else pop_next(ts, stack, r, nullptr);
+            }
+            if (ts.ref == REF_DONE) io.store(idx, h, r);
+        }
+    }
+}
+
+// Brute-force traversal for the naive layout (one thread per ray).
+template <bool ANY_HIT, class IO>
+__global__ void __launch_bounds__(128) k_trace_naive(const DeviceScene s, const IO io)
+{
+    const int64_t n = io.count();
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        TraversalRay r;
+        setup_ray(r, io.load(i));
+        Hit h;
+        h.tri = -1;
+        if (s.num_tris > 0) trace_naive<ANY_HIT>(s.tris_by_id, s.num_tris, r, h, nullptr);
+        io.store(i, h, r);
+    }
+}
+
+// Resident-grid size of a kernel (blocks of 128 threads), cached per kernel.
+int resident_blocks_of(const void* kernel);
+template <class K>
+int resident_blocks(K kernel)
+{
+    return resident_blocks_of(reinterpret_cast<const void*>(kernel));
+}
+
+// Launches the traversal for `io` on `stream`: persistent kernel for the
+// BVH layouts (with the scene's work counter reset first), brute force for
+// the naive layout. `max_rays` bounds the grid (0 = resident grid).
+template <bool ANY_HIT, int STACK, class IO>
+int launch_trace_stack(LmgpuScene* sc, const IO& io, int64_t max_rays, cudaStream_t stream)
+{
+    const DeviceScene& s = sc->dev;
+    if (s.layout == LMGPU_LAYOUT_NAIVE || s.num_tris == 0) {
+        const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((max_rays + 127) / 128, 148 * 64));
+        k_trace_naive<ANY_HIT, IO><<<blocks, 128, 0, stream>>>(s, io);
+        LMGPU_CUDA_TRY(cudaGetLastError());
+        return LMGPU_OK;
+    }
+    // Each launch takes its own counter from the scene's ring, so persistent
+    // kernels queued on different streams never share one.
+    unsigned long long* work = sc->d_work + (sc->work_slot++ % LmgpuScene::WORK_SLOTS);
+    LMGPU_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(unsigned long long), stream));
+    if (s.layout == LMGPU_LAYOUT_BVH2) {
+        auto k = k_trace_persistent<LMGPU_LAYOUT_BVH2, STACK, ANY_HIT, IO>;
+        int64_t blocks = resident_blocks(k);
+        if (max_rays > 0) blocks = std::max<int64_t>(1, std::min<int64_t>(blocks, (max_rays + 127) / 128));
+        k<<<blocks, 128, 0, stream>>>(s, io, sc->d_status, work);
+    } else {
+        auto k = k_trace_persistent<LMGPU_LAYOUT_BVH4, STACK, ANY_HIT, IO>;
+        int64_t blocks = resident_blocks(k);
+        if (max_rays > 0) blocks = std::max<int64_t>(1, std::min<int64_t>(blocks, (max_rays + 127) / 128));
+        k<<<blocks, 128, 0, stream>>>(s, io, sc->d_status, work);
+    }
+    LMGPU_CUDA_TRY(cudaGetLastError());
+    return LMGPU_OK;
+}
+
+template <bool ANY_HIT, class IO>
+int launch_trace(LmgpuScene* sc, const IO& io, int64_t max_rays, cudaStream_t stream)
+{
+    const int cap = sc->dev.stack_cap;
+    if (cap <= 32) return launch_trace_stack<ANY_HIT, 32>(sc, io, max_rays, stream);
+    if (cap <= 64) return launch_trace_stack<ANY_HIT, 64>(sc, io, max_rays, stream);
+    if (cap <= 128) return launch_trace_stack<ANY_HIT, 128>(sc, io, max_rays, stream);
+    if (cap <= 256) return launch_trace_stack<ANY_HIT, 256>(sc, io, max_rays, stream);
+    return fail(LMGPU_ERR_UNSUPPORTED, "BVH deeper than the largest compiled traversal stack (256)");
+}
+
+}  // namespace lmgpu

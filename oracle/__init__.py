@@ -180,3 +180,123 @@ def stub_random_mesh():
     n = np.zeros(9000, np.float32)
     ref("f").lmref_stub_random_mesh(_ptr(p), _ptr(n))
     return p.reshape(-1, 3), n.reshape(-1, 3)
+
+
+# ------------------------------------------------------------ rendering ----
+
+class _RefRenderDesc(ctypes.Structure):
+    _fields_ = [("num_prims", ctypes.c_int), ("positions", ctypes.POINTER(ctypes.c_void_p)),
+                ("normals", ctypes.POINTER(ctypes.c_void_p)), ("faces", ctypes.POINTER(ctypes.c_void_p)),
+                ("num_vertices", ctypes.c_void_p), ("num_faces", ctypes.c_void_p), ("material", ctypes.c_void_p),
+                ("light", ctypes.c_void_p), ("num_materials", ctypes.c_int), ("mat_type", ctypes.c_void_p),
+                ("mat_R", ctypes.c_void_p), ("num_lights", ctypes.c_int), ("light_Le", ctypes.c_void_p),
+                ("has_env", ctypes.c_int), ("env_Le", ctypes.c_float * 3), ("eye", ctypes.c_float * 3),
+                ("center", ctypes.c_float * 3), ("up", ctypes.c_float * 3), ("fovy", ctypes.c_float),
+                ("width", ctypes.c_int), ("height", ctypes.c_int), ("renderer", ctypes.c_char_p),
+                ("rr_depth", ctypes.c_int), ("max_path_vertices", ctypes.c_int), ("seed", ctypes.c_int),
+                ("num_samples", ctypes.c_longlong), ("num_threads", ctypes.c_int),
+                ("samples_per_block", ctypes.c_longlong)]
+
+
+def flatten_primitives(prims):
+    """World-space arrays of a lightmetrica_b200 Primitives description:
+    per primitive positions/normals/faces, material (type, R) and light
+    indices in first-use order, like the GPU scene description."""
+    out = {"pos": [], "nrm": [], "faces": [], "mat": [], "light": []}
+    mats, mat_index, lights, light_index = [], {}, [], {}
+    for p in prims.primitives:
+        m = p.mesh
+        pos = m.positions.astype(np.float64)
+        nrm = m.normals.astype(np.float64) if m.normals is not None else None
+        if p.transform is not None:
+            T = np.asarray(p.transform, np.float64).reshape(4, 4)
+            pos = pos @ T[:3, :3].T + T[:3, 3]
+            if nrm is not None:
+                nrm = nrm @ np.linalg.inv(T[:3, :3])
+        if nrm is None:
+            nrm = np.zeros_like(pos)
+            f = m.faces.astype(np.int64)
+            g = np.cross(pos[f[:, 1]] - pos[f[:, 0]], pos[f[:, 2]] - pos[f[:, 0]])
+            for c in range(3):
+                nrm[f[:, c]] = g
+        out["pos"].append(np.ascontiguousarray(pos, np.float32).reshape(-1))
+        out["nrm"].append(np.ascontiguousarray(nrm, np.float32).reshape(-1))
+        out["faces"].append(np.ascontiguousarray(m.faces, np.uint32).reshape(-1))
+        if p.bsdf is not None:
+            if id(p.bsdf) not in mat_index:
+                mat_index[id(p.bsdf)] = len(mats)
+                mats.append(p.bsdf)
+            out["mat"].append(mat_index[id(p.bsdf)])
+        else:
+            out["mat"].append(-1)
+        if p.light is not None:
+            if id(p.light) not in light_index:
+                light_index[id(p.light)] = len(lights)
+                lights.append(p.light)
+            out["light"].append(light_index[id(p.light)])
+        else:
+            out["light"].append(-1)
+    out["mats"] = mats
+    out["lights"] = lights
+    return out
+
+
+def ref_render(prims, renderer="pt", num_samples=None, spp=16, rr_depth=1, max_path_vertices=-1, seed=1,
+               threads=None, precision="d", samples_per_block=100):
+    """Renders `prims` with the reference's own renderer + `mt` scheduler
+    (oracle/_ref). Returns (film (H, W, 3) float32, render seconds)."""
+    L = ref(precision)
+    if not hasattr(L, "lmref_render"):
+        raise RuntimeError("reference harness built without the renderer")
+    L.lmref_render.restype = ctypes.c_double
+    L.lmref_render.argtypes = [ctypes.POINTER(_RefRenderDesc), ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+    fl = flatten_primitives(prims)
+    cam = prims.camera
+    W, H = cam.film.width, cam.film.height
+    n = len(prims.primitives)
+    keep = []
+
+    def ptrs(arrs):
+        a = (ctypes.c_void_p * n)(*[x.ctypes.data for x in arrs])
+        keep.append(a)
+        return a
+    nv = np.array([x.size // 3 for x in fl["pos"]], np.int32)
+    nf = np.array([x.size // 3 for x in fl["faces"]], np.int32)
+    mat = np.array(fl["mat"], np.int32)
+    lig = np.array(fl["light"], np.int32)
+    mt = np.array([m.kind for m in fl["mats"]] or [0], np.int32)
+    mR = np.array([np.broadcast_to(np.asarray(m.reflectance, np.float32), (3,)) for m in fl["mats"]] or [[0, 0, 0]],
+                  np.float32).reshape(-1)
+    lLe = np.array([np.broadcast_to(np.asarray(l.luminance, np.float32), (3,)) for l in fl["lights"]] or [[0, 0, 0]],
+                   np.float32).reshape(-1)
+    keep += [nv, nf, mat, lig, mt, mR, lLe]
+    d = _RefRenderDesc()
+    d.num_prims = n
+    d.positions = ptrs(fl["pos"])
+    d.normals = ptrs(fl["nrm"])
+    d.faces = ptrs(fl["faces"])
+    d.num_vertices, d.num_faces, d.material, d.light = nv.ctypes.data, nf.ctypes.data, mat.ctypes.data, lig.ctypes.data
+    d.num_materials = len(fl["mats"])
+    d.mat_type, d.mat_R = mt.ctypes.data, mR.ctypes.data
+    d.num_lights = len(fl["lights"])
+    d.light_Le = lLe.ctypes.data
+    if prims.environment_light is not None:
+        d.has_env = 1
+        le = np.broadcast_to(np.asarray(prims.environment_light.luminance, np.float32), (3,))
+        for c in range(3):
+            d.env_Le[c] = float(le[c])
+    for c in range(3):
+        d.eye[c], d.center[c], d.up[c] = cam.eye[c], cam.center[c], cam.up[c]
+    d.fovy = cam.fovy
+    d.width, d.height = W, H
+    d.renderer = renderer.encode()
+    d.rr_depth, d.max_path_vertices, d.seed = rr_depth, max_path_vertices, seed
+    d.num_samples = int(num_samples if num_samples is not None else spp * W * H)
+    d.num_threads = int(threads or os.cpu_count() or 1)
+    d.samples_per_block = samples_per_block
+    film = np.zeros((H, W, 3), np.float32)
+    bt = ctypes.c_double()
+    secs = L.lmref_render(ctypes.byref(d), film.ctypes.data, ctypes.byref(bt))
+    if secs < 0:
+        raise RuntimeError(f"reference render failed ({secs})")
+    return film, secs

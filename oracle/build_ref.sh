@@ -24,7 +24,7 @@ SRC="$REF/src/liblightmetrica"
 CORE="scene.cpp scene.bvh.cpp scene.naive.cpp object.cpp align.cpp"
 RENDER="pathtrace.cpp pathtrace.direct.cpp pathtrace.mis.cpp renderutils.cpp diffuse.cpp mirror.cpp \
         light.area.cpp light.env.const.cpp emittershape.sphere.cpp perspectivecamera.cpp \
-        randomsampler.cpp standardmtrand.cpp sched.mt.cpp constanttexture.cpp"
+        randomsampler.cpp standardmtrand.cpp sched.mt.cpp constanttexture.cpp hdrfilm.cpp bitmap.cpp"
 # The system g++ (the one whose libgomp is installed); override with LMREF_CXX.
 CXX="${LMREF_CXX:-/usr/bin/g++}"
 COMMON=(-std=c++14 -O2 -msse4.2 -mno-fma -fPIC -fopenmp -w

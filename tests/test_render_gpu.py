@@ -1,0 +1,105 @@
+"""Image parity of the GPU path tracer with the reference's own renderers.
+
+Oracle: the reference's pt.mis in double precision at 4096 spp
+(tests/golden/cornell_*_ref_mis_4096spp.npz, made by gen_golden.py from the
+reference sources). Metric: relMSE = mean((x - r)^2 / (r^2 + 1e-2)) over
+pixels and channels. The reference image alone carries relMSE ~1.6e-4 of
+Monte Carlo noise (two independent 1024-spp reference renders differ by
+1.3e-3), so the bar relMSE <= 1e-3 leaves room for the GPU estimate's own
+noise only; pt without next-event estimation needs 64x more samples for the
+same noise and is held to the same bar at 65,536 spp.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from lightmetrica_b200 import create_renderer, create_scheduler, create_scene, native, scenes
+
+pytestmark = pytest.mark.gpu
+
+RELMSE_BAR = 1e-3
+
+
+def relmse(x, r):
+    return float(np.mean((x - r) ** 2 / (r ** 2 + 1e-2)))
+
+
+def golden(golden_dir, variant):
+    return np.load(os.path.join(golden_dir, f"cornell_{variant}_ref_mis_4096spp.npz"))["film"]
+
+
+def render(prims, technique, spp, rr_depth=3, max_pv=9, seed=7, sampling="stratified", fp64=False, layout="bvh"):
+    scene = create_scene(layout)
+    scene.load(prims)
+    scene.configure({})
+    scene.build()
+    r = create_renderer(technique)
+    r.configure({"rr_depth": rr_depth, "max_path_vertices": max_pv, "sampler": {"rng_seed": seed, "sampling": sampling}})
+    W, H = prims.camera.film.width, prims.camera.film.height
+    s = create_scheduler("mt")
+    s.configure({"num_samples": W * H * spp, "film_fp64": fp64})
+    film = s.render(r, scene)
+    stats = s.last_stats
+    scene.close()
+    return film, stats
+
+
+@pytest.mark.parametrize("variant", ["classic", "mixed"])
+@pytest.mark.parametrize("technique,spp", [("pt.mis", 16384), ("pt.direct", 16384), ("pt", 65536)])
+def test_image_matches_reference(cuda, golden_dir, variant, technique, spp):
+    ref = golden(golden_dir, variant)
+    film, stats = render(scenes.cornell_box(128, 128, variant=variant), technique, spp)
+    e = relmse(film, ref)
+    print(f"{variant} {technique} {spp} spp: relMSE {e:.3e}, {stats['rays_traced'] / stats['device_ms'] / 1e3:.1f} Mrays/s")
+    assert np.isfinite(film).all()
+    assert e <= RELMSE_BAR, f"relMSE {e:.3e}"
+    np.testing.assert_allclose(film.mean(axis=(0, 1)), ref.mean(axis=(0, 1)), rtol=2e-2)
+
+
+def test_uniform_raster_sampling_matches_reference(cuda, golden_dir):
+    """The reference's own raster sampling (uniform over the film, pathtrace.cpp:168)."""
+    ref = golden(golden_dir, "classic")
+    film, _ = render(scenes.cornell_box(128, 128), "pt.mis", 16384, sampling="uniform")
+    assert relmse(film, ref) <= RELMSE_BAR
+
+
+def test_layouts_and_fp64_film_agree(cuda):
+    prims = scenes.cornell_box(64, 64, variant="mixed")
+    a, _ = render(prims, "pt.mis", 256, fp64=True)
+    b, _ = render(prims, "pt.mis", 256, fp64=False)
+    c, _ = render(prims, "pt.mis", 256, fp64=True, layout="qbvh")
+    # Same seed and samples: identical paths; only the film's summation order
+    # and precision differ.
+    np.testing.assert_allclose(a, b, rtol=1e-4, atol=1e-6)
+    np.testing.assert_allclose(a, c, rtol=1e-9, atol=1e-9)
+
+
+def test_max_path_vertices_edges(cuda):
+    prims = scenes.cornell_box(64, 64)
+    black, _ = render(prims, "pt", 16, max_pv=1)
+    assert not black.any()
+    # max_path_vertices = 2: only emitters seen directly; pt and pt.mis agree.
+    a, _ = render(prims, "pt", 4096, max_pv=2)
+    b, _ = render(prims, "pt.mis", 4096, max_pv=2)
+    assert a.max() > 1.0
+    np.testing.assert_allclose(a.sum(), b.sum(), rtol=2e-2)
+
+
+def test_render_errors_are_reported(cuda):
+    prims = scenes.cornell_box(32, 32)
+    prims.camera = None
+    scene = create_scene("bvh")
+    scene.load(prims)
+    scene.configure({})
+    scene.build()
+    r = create_renderer("pt")
+    r.configure({})
+    s = create_scheduler("mt")
+    s.configure({"num_samples": 1024})
+    with pytest.raises(RuntimeError):
+        s.render(r, scene)
+    with pytest.raises(ValueError):
+        s.configure({"num_samples": 0})
+    with pytest.raises(ValueError):
+        create_renderer("bpt")
