@@ -221,6 +221,34 @@ int lmgpu_render(LmgpuScene* scene, const LmgpuRenderParams* params,
 int lmgpu_render_device(LmgpuScene* scene, const LmgpuRenderParams* params,
                         void* film_device, void* stream, LmgpuRenderStats* stats);
 
+/* ---------------------------------------------------- differentiable ---- */
+
+/* Parameters of the differentiable render, DEVICE pointers (NULL = the
+ * scene's own values): per-triangle RGB albedo of diffuse BSDFs (3 floats per
+ * triangle, reference TriAccel numbering) and per-area-light RGB emission
+ * (3 floats per light). No reference counterpart: lightmetrica has no
+ * differentiable renderer; these extend its pt / pt.direct / pt.mis. */
+typedef struct {
+    const float* albedo;
+    const float* emission;
+} LmgpuDiffParams;
+
+/* Forward pass: renders `params` with `diff` into a DEVICE image (W*H*3,
+ * accumulated with atomics, already rescaled by W*H/num_samples; the caller
+ * zeroes it). Same estimator as lmgpu_render. */
+int lmgpu_adjoint_forward(LmgpuScene* scene, const LmgpuRenderParams* params,
+                          const LmgpuDiffParams* diff, float* image_device,
+                          void* stream, LmgpuRenderStats* stats);
+
+/* Adjoint pass: given dL/dimage (DEVICE, W*H*3, w.r.t. the rescaled image),
+ * replays every sample's path from its random-number counters and adds
+ * dL/d(albedo) (3 per triangle) and dL/d(emission) (3 per light) to the
+ * DEVICE gradient buffers (FP32 atomics; the caller zeroes them). */
+int lmgpu_adjoint_backward(LmgpuScene* scene, const LmgpuRenderParams* params,
+                           const LmgpuDiffParams* diff, const float* dL_dimage_device,
+                           float* d_albedo_device, float* d_emission_device,
+                           void* stream, LmgpuRenderStats* stats);
+
 /* ------------------------------------------------------------- misc ----- */
 const char* lmgpu_last_error(void);
 int lmgpu_abi_version(void);

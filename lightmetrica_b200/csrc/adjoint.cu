@@ -1,0 +1,385 @@
+// Differentiable rendering: a forward / adjoint pair over the path tracer
+// with per-triangle diffuse albedo and per-light emission as parameters.
+//
+// Both passes run the same per-sample path (the reference's pt / pt.direct /
+// pt.mis loops, pathtrace*.cpp) one thread per sample. The adjoint pass does
+// not store path vertices from the forward pass: it replays every path from
+// its counter-based random numbers (recomputation instead of checkpointing)
+// and, for each radiance contribution c splatted at pixel p, adds
+// dL/dI_p * c / R_t to the gradient of the albedo R of every diffuse vertex t
+// on the contribution's prefix (c is linear in each of them) and
+// dL/dI_p * c / Le to the emission of its light. Russian-roulette
+// probabilities and MIS weights are held at their sampled values, which keeps
+// the estimator unbiased for the diffuse BSDFs (their sampling densities do
+// not depend on R). Per-vertex records live in a fixed local array
+// (MAX_REPLAY_VERTS); longer paths flag LMGPU_ERR_QUEUE_OVERFLOW.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstring>
+
+#include "../../include/lmgpu.h"
+#include "internal.h"
+#include "pathtrace.cuh"
+#include "rng.cuh"
+#include "trace.cuh"
+#include "trace4.cuh"
+
+namespace lmgpu {
+namespace {
+
+constexpr int MAX_REPLAY_VERTS = 64;
+
+struct DiffConsts {
+    int32_t technique, rr_depth, max_pv, sampling;
+    uint64_t seed;
+    int64_t sample_offset, num_samples, pixels;
+    float scale;             // film rescale W*H/num_samples
+    const float* albedo;     // 3 per triangle or null
+    const float* emission;   // 3 per area light or null
+};
+
+template <int LAYOUT, bool ANY, int STACK>
+__device__ __forceinline__ int32_t cast_ray(const DeviceScene& s, V3 o, V3 d, float tmin, float tmax, Hit& h,
+                                            int2* stack, int32_t* status)
+{
+    RayIn in;
+    in.o[0] = o.x; in.o[1] = o.y; in.o[2] = o.z;
+    in.d[0] = d.x; in.d[1] = d.y; in.d[2] = d.z;
+    in.tmin = tmin; in.tmax = tmax;
+    TraversalRay r;
+    setup_ray(r, in);
+    h.tri = -1;
+    if (s.num_tris == 0) return -1;
+    bool ok;
+    if (LAYOUT == LMGPU_LAYOUT_BVH2) ok = trace_bvh2<ANY>(s.bvh2, s.tris, s.root_ref, s.root_box, r, h, stack, STACK, nullptr);
+    else if (LAYOUT == LMGPU_LAYOUT_BVH4) ok = trace_bvh4<ANY>(s.bvh4, s.tris, s.root_ref4, s.root_box, r, h, stack, STACK, nullptr);
+    else { trace_naive<ANY>(s.tris_by_id, s.num_tris, r, h, nullptr); ok = true; }
+    if (!ok) { atomicOr(status, STATUS_STACK_OVERFLOW); h.tri = -1; }
+    return h.tri;
+}
+
+template <int LAYOUT, int STACK>
+__device__ __forceinline__ bool visible(const DeviceScene& s, V3 a, V3 b, int2* stack, int32_t* status)
+{
+    const V3 d = b - a;
+    const float len = sqrtf(length2(d));
+    const V3 dn = d / len;
+    const float maxt = len * (1.0f - EPS_F);
+    Hit h;
+    if (cast_ray<LAYOUT, true, STACK>(s, a, dn, EPS_F, maxt, h, stack, status) >= 0) return false;
+    float t;
+    if (s.has_env && env_sphere_intersect(s, a, dn, EPS_F, maxt, t)) return false;
+    return true;
+}
+
+__device__ __forceinline__ Material diff_material(const DeviceScene& s, const DiffConsts& c, int tri)
+{
+    Material m = material_of(s, s.tri_prim[tri]);
+    if (c.albedo && m.type == LMGPU_BSDF_DIFFUSE) m.R = load3(c.albedo + 3 * (int64_t)tri);
+    return m;
+}
+
+__device__ __forceinline__ V3 light_Le(const DeviceScene& s, const DiffConsts& c, int li)
+{
+    if (li >= s.num_area_lights) return load3(s.env_Le);
+    return c.emission ? load3(c.emission + 3 * li) : load3(s.area_lights[li].Le);
+}
+
+struct Replay {
+    int32_t tri[MAX_REPLAY_VERTS];
+    int n;
+};
+
+// One contribution: forward splats it, the adjoint distributes dL/dI . c.
+template <bool BACKWARD>
+__device__ __forceinline__ void contribute(const DiffConsts& c, const DeviceScene& s, const Replay& rp, int depth,
+                                           int light, int pixel, V3 contrib, float* image, const float* dL,
+                                           float* d_albedo, float* d_emission)
+{
+    if (pixel < 0 || is_zero(contrib)) return;
+    if (!BACKWARD) {
+        atomicAdd(image + 3 * pixel, contrib.x * c.scale);
+        atomicAdd(image + 3 * pixel + 1, contrib.y * c.scale);
+        atomicAdd(image + 3 * pixel + 2, contrib.z * c.scale);
+        return;
+    }
+    const V3 w = v3(dL[3 * pixel] * contrib.x, dL[3 * pixel + 1] * contrib.y, dL[3 * pixel + 2] * contrib.z) * c.scale;
+    if (is_zero(w)) return;
+    for (int i = 0; i < depth && i < rp.n; i++) {
+        const int t = rp.tri[i];
+        const Material m = diff_material(s, c, t);
+        if (m.type != LMGPU_BSDF_DIFFUSE) continue;
+        if (m.R.x != 0.0f) atomicAdd(d_albedo + 3 * (int64_t)t, w.x / m.R.x);
+        if (m.R.y != 0.0f) atomicAdd(d_albedo + 3 * (int64_t)t + 1, w.y / m.R.y);
+        if (m.R.z != 0.0f) atomicAdd(d_albedo + 3 * (int64_t)t + 2, w.z / m.R.z);
+    }
+    if (light >= 0 && light < s.num_area_lights) {
+        const V3 Le = light_Le(s, c, light);
+        if (Le.x != 0.0f) atomicAdd(d_emission + 3 * light, w.x / Le.x);
+        if (Le.y != 0.0f) atomicAdd(d_emission + 3 * light + 1, w.y / Le.y);
+        if (Le.z != 0.0f) atomicAdd(d_emission + 3 * light + 2, w.z / Le.z);
+    }
+}
+
+// Light sample with the parameterised emission; returns the light index.
+__device__ __forceinline__ int sample_light_diff(const DeviceScene& s, const DiffConsts& c, float u0, float u1, LightPoint& lp)
+{
+    if (!sample_light(s, u0, u1, lp)) return -1;
+    const int nl = s.num_lights;
+    const int li = min(static_cast<int>(u0 * float(nl)), nl - 1);
+    lp.Le = light_Le(s, c, li);
+    return li;
+}
+
+template <int TECH, int LAYOUT, int STACK, bool BACKWARD>
+__global__ void __launch_bounds__(128) k_diff(const DeviceScene s, const DiffConsts c, float* image, const float* dL,
+                                              float* d_albedo, float* d_emission, int32_t* status)
+{
+    int2 stack[STACK];
+    Replay rp;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < c.num_samples; j += stride) {
+        const uint64_t sample = (uint64_t)(c.sample_offset + j);
+        const uint64_t key = sample_key(c.seed, sample);
+        rp.n = 0;
+        const float u0 = rng_uniform(key, DIM_RASTER), u1 = rng_uniform(key, DIM_RASTER + 1);
+        float rx, ry;
+        if (c.sampling == LMGPU_SAMPLING_STRATIFIED) {
+            const int64_t pix = (int64_t)(sample % (uint64_t)c.pixels);
+            rx = (float(pix % s.cam.width) + u0) / float(s.cam.width);
+            ry = (float(pix / s.cam.width) + u1) / float(s.cam.height);
+        } else {
+            rx = u0; ry = u1;
+        }
+        const int path_pixel = film_pixel(s.cam, rx, ry);
+        float pdf_cam;
+        const V3 dir = camera_direction(s.cam, rx, ry, pdf_cam);
+        const V3 cp = load3(s.cam.position);
+        V3 thr = v3(1, 1, 1);
+        if (c.max_pv != -1 && c.max_pv <= 1) continue;
+        V3 prev_p = cp, prev_n = v3(0, 0, 1);
+        bool prev_deg = true, prev_spec = false;
+        float prev_pdf = pdf_cam;
+        float tmin = TECH == LMGPU_RENDER_PT ? 0.0f : EPS_F;
+        bool alive = true;
+        if (TECH != LMGPU_RENDER_PT) {
+            LightPoint lp;
+            const int li = sample_light_diff(s, c, rng_uniform(key, dim_vertex(1) + DIM_LIGHT),
+                                             rng_uniform(key, dim_vertex(1) + DIM_LIGHT + 1), lp);
+            if (li >= 0) {
+                const V3 ppL = normalize(lp.p - cp);
+                float lrx, lry, We;
+                if (camera_project(s.cam, cp, ppL, lrx, lry, We) && We > 0.0f) {
+                    const float G = geometry_term(cp, v3(0, 0, 1), true, lp.p, lp.n, false);
+                    const V3 Le = emitted(lp.Le, lp.n, -ppL);
+                    if (G != 0.0f && !is_zero(Le) && visible<LAYOUT, STACK>(s, cp, lp.p, stack, status)) {
+                        float w = 1.0f;
+                        if (TECH == LMGPU_RENDER_PT_MIS) { const float pdl = lp.pdf_area / G; w = pdl / (pdl + We); }
+                        contribute<BACKWARD>(c, s, rp, 0, li, film_pixel(s.cam, lrx, lry), Le * (w * We * G / lp.pdf_area),
+                                             image, dL, d_albedo, d_emission);
+                    }
+                }
+            }
+            if (c.rr_depth != -1 && 1 >= c.rr_depth) {
+                const float p = fminf(0.5f, luminance(thr));
+                if (rng_uniform(key, dim_vertex(1) + DIM_RR) > p) alive = false;
+                else thr = thr / p;
+            }
+        }
+        V3 ro = cp, rd = dir;
+        for (int k = 1; alive; k++) {
+            if (c.max_pv != -1 && k >= c.max_pv) break;
+            Hit h;
+            const int tri = cast_ray<LAYOUT, false, STACK>(s, ro, rd, tmin, FLT_MAX, h, stack, status);
+            Geom g;
+            const V3 wi = -rd;
+            V3 Le = v3(0, 0, 0);
+            float lpdf = 0.0f;
+            int light = -1;
+            bool surface = false;
+            Material m;
+            m.type = LMGPU_BSDF_BLACK;
+            m.R = v3(0, 0, 0);
+            if (tri < 0) {
+                float t;
+                if (!(s.has_env && env_sphere_intersect(s, ro, rd, tmin, FLT_MAX, t))) break;
+                env_surface(s, ro, rd, t, g);
+                Le = emitted(load3(s.env_Le), g.sn, wi);
+                lpdf = s.env_inv_area;
+                light = s.num_area_lights;
+            } else {
+                surface_from_hit(s, tri, h.u, h.v, ro, rd, h.t, g);
+                const int li = s.prim_light[s.tri_prim[tri]];
+                if (li >= 0) {
+                    Le = emitted(light_Le(s, c, li), g.sn, wi);
+                    lpdf = s.area_lights[li].inv_area;
+                    light = li;
+                }
+                m = diff_material(s, c, tri);
+                surface = true;
+                if (rp.n < MAX_REPLAY_VERTS) rp.tri[rp.n++] = tri;
+                else { atomicOr(status, STATUS_QUEUE_OVERFLOW); break; }
+            }
+            const int depth_here = rp.n - (surface ? 1 : 0);
+            if (!is_zero(Le)) {
+                const V3 contrib = thr * Le;
+                if (TECH == LMGPU_RENDER_PT || prev_spec) {
+                    contribute<BACKWARD>(c, s, rp, depth_here, light, path_pixel, contrib, image, dL, d_albedo, d_emission);
+                } else if (TECH == LMGPU_RENDER_PT_MIS) {
+                    const float G = geometry_term(prev_p, prev_n, prev_deg, g.p, g.sn, false);
+                    const float pdl = G == 0.0f ? 0.0f : lpdf / (float(s.num_lights) * G);
+                    contribute<BACKWARD>(c, s, rp, depth_here, light, path_pixel, contrib * (prev_pdf / (prev_pdf + pdl)),
+                                         image, dL, d_albedo, d_emission);
+                }
+            }
+            if (!surface) break;
+            const int v = k + 1;
+            if (TECH != LMGPU_RENDER_PT && c.max_pv != -1 && v >= c.max_pv) break;
+            if (TECH != LMGPU_RENDER_PT && has_non_delta(m.type)) {
+                LightPoint lp;
+                const int li = sample_light_diff(s, c, rng_uniform(key, dim_vertex(v) + DIM_LIGHT),
+                                                 rng_uniform(key, dim_vertex(v) + DIM_LIGHT + 1), lp);
+                if (li >= 0) {
+                    const V3 ppL = normalize(lp.p - g.p);
+                    float pb;
+                    const V3 fs = eval_bsdf(m, g, wi, ppL, pb);
+                    const float G = geometry_term(g.p, g.sn, false, lp.p, lp.n, false);
+                    const V3 Lel = emitted(lp.Le, lp.n, -ppL);
+                    if (G != 0.0f && !is_zero(fs) && !is_zero(Lel) && visible<LAYOUT, STACK>(s, g.p, lp.p, stack, status)) {
+                        float w = 1.0f;
+                        if (TECH == LMGPU_RENDER_PT_MIS) { const float pdl = lp.pdf_area / G; w = pdl / (pdl + pb); }
+                        contribute<BACKWARD>(c, s, rp, rp.n, li, path_pixel, thr * fs * Lel * (w * G / lp.pdf_area),
+                                             image, dL, d_albedo, d_emission);
+                    }
+                }
+            }
+            const int kv = TECH == LMGPU_RENDER_PT ? k : v;
+            if (TECH != LMGPU_RENDER_PT && c.rr_depth != -1 && kv >= c.rr_depth) {
+                const float p = fminf(0.5f, luminance(thr));
+                if (rng_uniform(key, dim_vertex(kv) + DIM_RR) > p) break;
+                thr = thr / p;
+            }
+            const BsdfSample bs = sample_bsdf(m, g, wi, rng_uniform(key, dim_vertex(kv) + DIM_BSDF),
+                                              rng_uniform(key, dim_vertex(kv) + DIM_BSDF + 1),
+                                              rng_uniform(key, dim_vertex(kv) + DIM_COMP));
+            if (is_zero(bs.weight)) break;
+            thr = thr * bs.weight;
+            if (TECH == LMGPU_RENDER_PT && c.rr_depth != -1 && k >= c.rr_depth) {
+                const float p = fminf(0.5f, luminance(thr));
+                if (rng_uniform(key, dim_vertex(k) + DIM_RR) > p) break;
+                thr = thr / p;
+            }
+            if (TECH == LMGPU_RENDER_PT && c.max_pv != -1 && k + 1 >= c.max_pv) break;
+            prev_p = g.p; prev_n = g.sn; prev_deg = false; prev_spec = bs.specular; prev_pdf = bs.pdf;
+            ro = g.p; rd = bs.wo; tmin = EPS_F;
+        }
+    }
+}
+
+template <int TECH, int LAYOUT, int STACK>
+int launch_diff_l(LmgpuScene* sc, const DiffConsts& c, bool backward, float* image, const float* dL, float* da,
+                  float* de, cudaStream_t st)
+{
+    const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((c.num_samples + 127) / 128, 148 * 16));
+    if (backward) k_diff<TECH, LAYOUT, STACK, true><<<blocks, 128, 0, st>>>(sc->dev, c, image, dL, da, de, sc->d_status);
+    else k_diff<TECH, LAYOUT, STACK, false><<<blocks, 128, 0, st>>>(sc->dev, c, image, dL, da, de, sc->d_status);
+    LMGPU_CUDA_TRY(cudaGetLastError());
+    return LMGPU_OK;
+}
+
+template <int TECH, int STACK>
+int launch_diff_s(LmgpuScene* sc, const DiffConsts& c, bool backward, float* image, const float* dL, float* da,
+                  float* de, cudaStream_t st)
+{
+    switch (sc->dev.layout) {
+    case LMGPU_LAYOUT_BVH2: return launch_diff_l<TECH, LMGPU_LAYOUT_BVH2, STACK>(sc, c, backward, image, dL, da, de, st);
+    case LMGPU_LAYOUT_BVH4: return launch_diff_l<TECH, LMGPU_LAYOUT_BVH4, STACK>(sc, c, backward, image, dL, da, de, st);
+    default: return launch_diff_l<TECH, LMGPU_LAYOUT_NAIVE, 1>(sc, c, backward, image, dL, da, de, st);
+    }
+}
+
+template <int TECH>
+int launch_diff_t(LmgpuScene* sc, const DiffConsts& c, bool backward, float* image, const float* dL, float* da,
+                  float* de, cudaStream_t st)
+{
+    const int cap = sc->dev.stack_cap;
+    if (cap <= 32) return launch_diff_s<TECH, 32>(sc, c, backward, image, dL, da, de, st);
+    if (cap <= 64) return launch_diff_s<TECH, 64>(sc, c, backward, image, dL, da, de, st);
+    if (cap <= 128) return launch_diff_s<TECH, 128>(sc, c, backward, image, dL, da, de, st);
+    return fail(LMGPU_ERR_UNSUPPORTED, "BVH too deep for the differentiable path (stack 128)");
+}
+
+int launch_diff(LmgpuScene* sc, const LmgpuRenderParams* p, const LmgpuDiffParams* dp, bool backward, float* image,
+                const float* dL, float* da, float* de, cudaStream_t st, LmgpuRenderStats* stats)
+{
+    if (!sc || !p) return fail(LMGPU_ERR_INVALID, "null argument");
+    if (!sc->dev.cam.valid) return fail(LMGPU_ERR_INVALID, "scene has no camera");
+    if (p->num_samples <= 0) return fail(LMGPU_ERR_INVALID, "num_samples must be positive");
+    if (p->technique < LMGPU_RENDER_PT || p->technique > LMGPU_RENDER_PT_MIS) return fail(LMGPU_ERR_INVALID, "unknown technique");
+    DiffConsts c;
+    std::memset(&c, 0, sizeof(c));
+    c.technique = p->technique;
+    c.rr_depth = p->rr_depth;
+    c.max_pv = p->max_path_vertices;
+    c.sampling = p->sampling;
+    c.seed = p->seed;
+    c.sample_offset = p->sample_offset;
+    c.num_samples = p->num_samples;
+    c.pixels = (int64_t)sc->dev.cam.width * sc->dev.cam.height;
+    c.scale = float(double(c.pixels) / double(p->num_samples));
+    c.albedo = dp ? dp->albedo : nullptr;
+    c.emission = dp ? dp->emission : nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (stats) {
+        LMGPU_CUDA_TRY(cudaEventCreate(&e0));
+        LMGPU_CUDA_TRY(cudaEventCreate(&e1));
+        LMGPU_CUDA_TRY(cudaEventRecord(e0, st));
+    }
+    int rc;
+    switch (p->technique) {
+    case LMGPU_RENDER_PT: rc = launch_diff_t<LMGPU_RENDER_PT>(sc, c, backward, image, dL, da, de, st); break;
+    case LMGPU_RENDER_PT_DIRECT: rc = launch_diff_t<LMGPU_RENDER_PT_DIRECT>(sc, c, backward, image, dL, da, de, st); break;
+    default: rc = launch_diff_t<LMGPU_RENDER_PT_MIS>(sc, c, backward, image, dL, da, de, st); break;
+    }
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->paths = p->num_samples;
+        if (rc == LMGPU_OK) {
+            cudaEventRecord(e1, st);
+            cudaEventSynchronize(e1);
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            stats->device_ms = ms;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    return rc;
+}
+
+}  // namespace
+}  // namespace lmgpu
+
+using namespace lmgpu;
+
+extern "C" {
+
+int lmgpu_adjoint_forward(LmgpuScene* scene, const LmgpuRenderParams* params, const LmgpuDiffParams* diff,
+                          float* image_device, void* stream, LmgpuRenderStats* stats)
+{
+    if (!image_device) return fail(LMGPU_ERR_INVALID, "null image");
+    return launch_diff(scene, params, diff, false, image_device, nullptr, nullptr, nullptr,
+                       static_cast<cudaStream_t>(stream), stats);
+}
+
+int lmgpu_adjoint_backward(LmgpuScene* scene, const LmgpuRenderParams* params, const LmgpuDiffParams* diff,
+                           const float* dL_dimage_device, float* d_albedo_device, float* d_emission_device,
+                           void* stream, LmgpuRenderStats* stats)
+{
+    if (!dL_dimage_device || !d_albedo_device || !d_emission_device)
+        return fail(LMGPU_ERR_INVALID, "null gradient buffer");
+    return launch_diff(scene, params, diff, true, nullptr, dL_dimage_device, d_albedo_device, d_emission_device,
+                       static_cast<cudaStream_t>(stream), stats);
+}
+
+}  // extern "C"

@@ -83,6 +83,10 @@ class RenderParams(ctypes.Structure):
                 ("sample_offset", c_int64), ("film_fp64", c_int32), ("wave_paths", c_int32)]
 
 
+class DiffParams(ctypes.Structure):
+    _fields_ = [("albedo", c_void_p), ("emission", c_void_p)]
+
+
 class RenderStats(ctypes.Structure):
     _fields_ = [("rays_traced", c_int64), ("shadow_rays", c_int64), ("paths", c_int64),
                 ("waves", c_int32), ("max_bounces_run", c_int32), ("device_ms", c_double)]
@@ -103,6 +107,9 @@ SIGNATURES = {
     "lmgpu_render": (c_int32, [c_void_p, P(RenderParams), c_void_p, P(RenderStats)]),
     "lmgpu_render_device": (c_int32, [c_void_p, P(RenderParams), c_void_p, c_void_p, P(RenderStats)]),
     "lmgpu_scene_status": (c_int32, [c_void_p, c_void_p]),
+    "lmgpu_adjoint_forward": (c_int32, [c_void_p, P(RenderParams), P(DiffParams), c_void_p, c_void_p, P(RenderStats)]),
+    "lmgpu_adjoint_backward": (c_int32, [c_void_p, P(RenderParams), P(DiffParams), c_void_p, c_void_p, c_void_p,
+                                         c_void_p, P(RenderStats)]),
     "lmgpu_intersect_counted": (c_int32, [c_void_p, P(RaysSoA), c_int64, P(HitsSoA), c_void_p, c_void_p]),
 }
 

@@ -300,3 +300,126 @@ def ref_render(prims, renderer="pt", num_samples=None, spp=16, rr_depth=1, max_p
     if secs < 0:
         raise RuntimeError(f"reference render failed ({secs})")
     return film, secs
+
+
+class _OrcPtDesc(ctypes.Structure):
+    _fields_ = [("num_tris", ctypes.c_int), ("pos", ctypes.c_void_p), ("nrm", ctypes.c_void_p),
+                ("tri_mat", ctypes.c_void_p), ("tri_light", ctypes.c_void_p), ("num_mats", ctypes.c_int),
+                ("mat_type", ctypes.c_void_p), ("mat_R", ctypes.c_void_p), ("tri_albedo", ctypes.c_void_p),
+                ("num_lights", ctypes.c_int), ("light_Le", ctypes.c_void_p), ("has_env", ctypes.c_int),
+                ("env_Le", ctypes.c_float * 3), ("eye", ctypes.c_float * 3), ("center", ctypes.c_float * 3),
+                ("up", ctypes.c_float * 3), ("fovy", ctypes.c_float), ("width", ctypes.c_int),
+                ("height", ctypes.c_int), ("technique", ctypes.c_int), ("rr_depth", ctypes.c_int),
+                ("max_pv", ctypes.c_int), ("sampling", ctypes.c_int), ("seed", ctypes.c_uint64),
+                ("sample_begin", ctypes.c_int64), ("sample_end", ctypes.c_int64)]
+
+
+_TECH = {"pt": 0, "pt.direct": 1, "pt.mis": 2}
+
+
+def _pt_desc(prims, technique, rr_depth, max_path_vertices, seed, sampling, tri_albedo, light_Le):
+    fl = flatten_primitives(prims)
+    pos, nrm, tmat, tlight = [], [], [], []
+    for k in range(len(fl["pos"])):
+        P = fl["pos"][k].reshape(-1, 3)
+        Nn = fl["nrm"][k].reshape(-1, 3)
+        F = fl["faces"][k].reshape(-1, 3).astype(np.int64)
+        pos.append(P[F].reshape(-1))
+        nrm.append(Nn[F].reshape(-1))
+        tmat.append(np.full(F.shape[0], fl["mat"][k], np.int32))
+        tlight.append(np.full(F.shape[0], fl["light"][k], np.int32))
+    keep = dict(pos=np.ascontiguousarray(np.concatenate(pos), np.float32),
+                nrm=np.ascontiguousarray(np.concatenate(nrm), np.float32),
+                tmat=np.concatenate(tmat), tlight=np.concatenate(tlight),
+                mt=np.array([m.kind for m in fl["mats"]] or [0], np.int32),
+                mR=np.array([np.broadcast_to(np.asarray(m.reflectance, np.float32), (3,)) for m in fl["mats"]]
+                            or [[0, 0, 0]], np.float32).reshape(-1))
+    if light_Le is None:
+        light_Le = np.array([np.broadcast_to(np.asarray(l.luminance, np.float32), (3,)) for l in fl["lights"]]
+                            or [[0, 0, 0]], np.float32)
+    keep["lLe"] = np.ascontiguousarray(light_Le, np.float32).reshape(-1)
+    if tri_albedo is not None:
+        keep["alb"] = np.ascontiguousarray(tri_albedo, np.float32).reshape(-1)
+    d = _OrcPtDesc()
+    d.num_tris = keep["tmat"].size
+    d.pos, d.nrm = keep["pos"].ctypes.data, keep["nrm"].ctypes.data
+    d.tri_mat, d.tri_light = keep["tmat"].ctypes.data, keep["tlight"].ctypes.data
+    d.num_mats = len(fl["mats"])
+    d.mat_type, d.mat_R = keep["mt"].ctypes.data, keep["mR"].ctypes.data
+    d.tri_albedo = keep["alb"].ctypes.data if "alb" in keep else None
+    d.num_lights = len(fl["lights"])
+    d.light_Le = keep["lLe"].ctypes.data
+    if prims.environment_light is not None:
+        d.has_env = 1
+        le = np.broadcast_to(np.asarray(prims.environment_light.luminance, np.float32), (3,))
+        for c in range(3):
+            d.env_Le[c] = float(le[c])
+    cam = prims.camera
+    for c in range(3):
+        d.eye[c], d.center[c], d.up[c] = cam.eye[c], cam.center[c], cam.up[c]
+    d.fovy = cam.fovy
+    d.width, d.height = cam.film.width, cam.film.height
+    d.technique = _TECH[technique]
+    d.rr_depth, d.max_pv = rr_depth, max_path_vertices
+    d.sampling = 0 if sampling == "stratified" else 1
+    d.seed = seed
+    return d, keep
+
+
+def _split_run(fn, d, total, threads, out_arrays):
+    """Runs fn(desc copy, *per-thread outputs) over [0, total) samples on
+    `threads` Python threads (ctypes releases the GIL) and sums the outputs."""
+    import threading
+    threads = max(1, min(threads or os.cpu_count() or 1, total))
+    parts = [[np.zeros_like(a, dtype=np.float64) for a in out_arrays] for _ in range(threads)]
+    descs = []
+    for t in range(threads):
+        dd = _OrcPtDesc()
+        ctypes.pointer(dd)[0] = d
+        dd.sample_begin = total * t // threads
+        dd.sample_end = total * (t + 1) // threads
+        descs.append(dd)
+    ths = [threading.Thread(target=fn, args=(descs[t], parts[t])) for t in range(threads)]
+    for th in ths:
+        th.start()
+    for th in ths:
+        th.join()
+    return [sum(p[i] for p in parts) for i in range(len(out_arrays))]
+
+
+def oracle_render(prims, technique="pt.mis", spp=16, rr_depth=1, max_path_vertices=-1, seed=1,
+                  sampling="stratified", threads=None, tri_albedo=None, light_Le=None):
+    """The C restatement's render (double), rescaled like the reference film:
+    (H, W, 3) float64."""
+    L = lib()
+    L.orc_render.restype = ctypes.c_int64
+    L.orc_render.argtypes = [ctypes.POINTER(_OrcPtDesc), ctypes.c_void_p]
+    d, keep = _pt_desc(prims, technique, rr_depth, max_path_vertices, seed, sampling, tri_albedo, light_Le)
+    W, H = prims.camera.film.width, prims.camera.film.height
+    total = W * H * spp
+
+    def run(dd, outs):
+        L.orc_render(ctypes.byref(dd), outs[0].ctypes.data)
+    film, = _split_run(run, d, total, threads, [np.zeros(W * H * 3)])
+    return (film * (W * H / total)).reshape(H, W, 3)
+
+
+def oracle_grad(prims, dL_dimage, technique="pt.mis", spp=16, rr_depth=1, max_path_vertices=-1, seed=1,
+                sampling="stratified", threads=None, tri_albedo=None, light_Le=None):
+    """FP64 reference gradient of a loss with image gradient dL_dimage
+    ((H, W, 3), w.r.t. the rescaled film) w.r.t. per-triangle albedo and
+    area-light emission: returns (d_albedo (T, 3), d_Le (lights, 3))."""
+    L = lib()
+    L.orc_render_grad.restype = ctypes.c_int64
+    L.orc_render_grad.argtypes = [ctypes.POINTER(_OrcPtDesc), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    d, keep = _pt_desc(prims, technique, rr_depth, max_path_vertices, seed, sampling, tri_albedo, light_Le)
+    W, H = prims.camera.film.width, prims.camera.film.height
+    total = W * H * spp
+    g = np.ascontiguousarray(np.asarray(dL_dimage, np.float64).reshape(-1) * (W * H / total))
+    T = d.num_tris
+    nl = max(1, d.num_lights)
+
+    def run(dd, outs):
+        L.orc_render_grad(ctypes.byref(dd), g.ctypes.data, outs[0].ctypes.data, outs[1].ctypes.data)
+    ga, gl = _split_run(run, d, total, threads, [np.zeros(3 * T), np.zeros(3 * nl)])
+    return ga.reshape(T, 3), gl.reshape(nl, 3)[:d.num_lights]

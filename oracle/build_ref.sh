@@ -7,7 +7,8 @@
 #   oracle/_ref/liblmref_f.so   (Math::Float = float,  LM_USE_SINGLE_PRECISION)
 #   oracle/_ref/liblmref_d.so   (Math::Float = double, LM_USE_DOUBLE_PRECISION)
 # Flags follow the reference's CMakeLists.txt:300-313 for GCC (-msse4.2,
-# -mno-fma); the QBVH source needs -fno-strict-aliasing on GCC 13, without it
+# -mno-fma) and its default Release build type (CMakeLists.txt:55-56, NDEBUG);
+# the QBVH source needs -fno-strict-aliasing on GCC 13, without it
 # it returns no hits. Nothing is written outside oracle/_ref.
 #
 # Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
@@ -27,9 +28,11 @@ RENDER="pathtrace.cpp pathtrace.direct.cpp pathtrace.mis.cpp renderutils.cpp dif
         randomsampler.cpp standardmtrand.cpp sched.mt.cpp constanttexture.cpp hdrfilm.cpp bitmap.cpp"
 # The system g++ (the one whose libgomp is installed); override with LMREF_CXX.
 CXX="${LMREF_CXX:-/usr/bin/g++}"
-COMMON=(-std=c++14 -O2 -msse4.2 -mno-fma -fPIC -fopenmp -w
+# -fno-gnu-unique: the float and double builds are loaded into one process, and
+# template statics (component registration) must stay per library.
+COMMON=(-std=c++14 -O2 -msse4.2 -mno-fma -fPIC -fopenmp -w -fno-gnu-unique
         -include cstdint -include stdexcept -include cstring -include cmath
-        -I"$HERE/shim" -I"$REF/include" -I"$SRC" -I"$REF/pch" -DLM_EXPORTS)
+        -I"$HERE/shim" -I"$REF/include" -I"$SRC" -I"$REF/pch" -DLM_EXPORTS -DNDEBUG)
 
 build_one() {  # $1 = f|d
   local tag="$1" prec objdir

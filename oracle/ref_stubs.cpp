@@ -35,12 +35,12 @@ unsigned int Logger::Indentation() { return 0; }
 void Logger::SetIndentation(unsigned int) {}
 
 // ------------------------------------------------------ ComponentFactory ----
-namespace {
 std::map<std::string, ComponentFactory::CreateComponentFunc>& Registry()
 {
 	static std::map<std::string, ComponentFactory::CreateComponentFunc> r;
 	return r;
 }
+namespace {
 std::string Key(const std::string& i, const std::string& t) { return i + "::" + t; }
 }
 
@@ -201,3 +201,12 @@ bool PluginManager::Register(const std::string& interfaceType, const std::string
 	return ComponentFactory::Register(interfaceType, implType, func);
 }
 LM_NAMESPACE_END
+
+// Diagnostics: the registered component keys ("interface::impl"), newline-separated.
+extern "C" const char* lmref_registered_components()
+{
+	static std::string out;
+	out.clear();
+	for (auto& kv : lightmetrica::Registry()) out += kv.first + "\n";
+	return out.c_str();
+}

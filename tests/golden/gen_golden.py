@@ -16,9 +16,10 @@ Fixtures:
                            reference BVHScene tri ids, t and (u, v)
   soup_duplicates.npz      1024 triangles, each repeated three times (exact
                            ties), 4096 rays; reference bvh and naive ids and t
-  cornell_{classic,mixed}_ref_mis_4096spp.npz
+  cornell_{classic,mixed}_ref_mis.npz
                            the reference's double-precision pt.mis image of
-                           lightmetrica_b200.scenes.cornell_box(128, 128, variant)
+                           lightmetrica_b200.scenes.cornell_box(128, 128,
+                           variant) (4096 / 16384 spp)
 Each fixture stores the inputs with the reference outputs for every scene
 type the reference builds here (bvh, qbvh, naive).
 """
@@ -130,18 +131,24 @@ def main():
     print("wrote soup_duplicates.npz hits", int((out["bvh_tri_id"] >= 0).sum()))
 
 
-def images():
+IMAGE_SPP = {"classic": 4096, "mixed": 16384}
+
+
+def images(variants=("classic", "mixed")):
     """Image oracles: the reference's own pt.mis in double precision
-    (oracle/_ref/liblmref_d.so) at 4096 samples per pixel on average
-    (uniform raster sampling, `mt` scheduler), 128 x 128, max_path_vertices 9
-    (max depth 8), rr_depth 3, rng standardmt seed 1."""
+    (oracle/_ref/liblmref_d.so), 128 x 128, max_path_vertices 9 (max depth
+    8), rr_depth 3, rng standardmt seed 1, uniform raster sampling with the
+    `mt` scheduler, at IMAGE_SPP samples per pixel on average (the mixed
+    scene's mirror caustics carry ~4x the per-sample variance, so it gets 4x
+    the samples)."""
     from lightmetrica_b200 import scenes
-    for variant in ("classic", "mixed"):
+    for variant in variants:
+        spp = IMAGE_SPP[variant]
         prims = scenes.cornell_box(128, 128, variant=variant)
-        film, secs = oracle.ref_render(prims, "pt.mis", spp=4096, rr_depth=3, max_path_vertices=9, seed=1)
-        np.savez_compressed(os.path.join(OUT, f"cornell_{variant}_ref_mis_4096spp.npz"), film=film,
-                            spp=4096, rr_depth=3, max_path_vertices=9, seconds=secs)
-        print("wrote", variant, "image", f"{secs:.1f} s", film.mean(axis=(0, 1)))
+        film, secs = oracle.ref_render(prims, "pt.mis", spp=spp, rr_depth=3, max_path_vertices=9, seed=1)
+        np.savez_compressed(os.path.join(OUT, f"cornell_{variant}_ref_mis.npz"), film=film,
+                            spp=spp, rr_depth=3, max_path_vertices=9, seconds=secs)
+        print("wrote", variant, "image", f"{spp} spp {secs:.1f} s", film.mean(axis=(0, 1)))
 
 
 if __name__ == "__main__":

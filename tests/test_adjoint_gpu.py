@@ -1,0 +1,140 @@
+"""Adjoint path replay (lmgpu_adjoint_forward / _backward) against central
+finite differences (h = 1e-3, common random numbers) and against the FP64
+CPU reference gradient of the oracle (same random numbers, same paths).
+The torch.autograd.Function below exists only in this test harness.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from lightmetrica_b200 import create_renderer, create_scene, scenes
+from lightmetrica_b200.diff import DifferentiableRender, light_emission, triangle_albedo
+
+pytestmark = pytest.mark.gpu
+
+RR_DEPTH, MAX_PV = 3, 9
+
+
+def setup(prims, technique="pt.mis", spp=64, seed=11, rr_depth=RR_DEPTH):
+    scene = create_scene("bvh")
+    scene.load(prims)
+    scene.configure({})
+    scene.build()
+    r = create_renderer(technique)
+    r.configure({"rr_depth": rr_depth, "max_path_vertices": MAX_PV, "sampler": {"rng_seed": seed}})
+    W, H = prims.camera.film.width, prims.camera.film.height
+    return scene, DifferentiableRender(scene, r, W * H * spp)
+
+
+def make_autograd(dr):
+    import torch
+
+    class LmgpuRenderFunction(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, albedo, emission):
+            ctx.save_for_backward(albedo, emission)
+            return dr.forward(albedo, emission)
+
+        @staticmethod
+        def backward(ctx, grad_image):
+            albedo, emission = ctx.saved_tensors
+            return dr.backward(albedo, emission, grad_image)
+    return LmgpuRenderFunction.apply
+
+
+def test_forward_matches_renderer(cuda):
+    import torch
+    from lightmetrica_b200 import create_scheduler
+    prims = scenes.cornell_box(64, 64, variant="mixed")
+    scene, dr = setup(prims, spp=64)
+    alb = torch.from_numpy(triangle_albedo(prims)).to(cuda)
+    em = torch.from_numpy(light_emission(prims)).to(cuda)
+    img = dr.forward(alb, em).cpu().numpy()
+    s = create_scheduler("mt")
+    s.configure({"num_samples": 64 * 64 * 64})
+    film = s.render(dr.renderer, scene)
+    # Same estimator, same random numbers: identical paths, only the
+    # atomic summation order differs.
+    np.testing.assert_allclose(img, film, rtol=1e-3, atol=1e-5)
+
+
+@pytest.mark.parametrize("technique", ["pt.mis", "pt.direct", "pt"])
+def test_gradient_matches_fp64_oracle(cuda, technique):
+    import torch
+    prims = scenes.cornell_box(32, 32)
+    spp = 32
+    scene, dr = setup(prims, technique, spp=spp)
+    alb0 = triangle_albedo(prims)
+    em0 = light_emission(prims)
+    rng = np.random.default_rng(4)
+    target_alb = np.clip(alb0 * rng.uniform(0.6, 1.4, alb0.shape), 0.05, 0.95).astype(np.float32)
+    alb = torch.from_numpy(alb0).to(cuda)
+    em = torch.from_numpy(em0).to(cuda)
+    target = dr.forward(torch.from_numpy(target_alb).to(cuda), em)
+    img = dr.forward(alb, em)
+    dL = 2.0 * (img - target)
+    da, de = dr.backward(alb, em, dL)
+    ga, gl = oracle.oracle_grad(prims, dL.cpu().numpy(), technique, spp=spp, rr_depth=RR_DEPTH,
+                                max_path_vertices=MAX_PV, seed=11, tri_albedo=alb0, threads=8)
+    da = da.cpu().numpy()
+    de = de.cpu().numpy()
+    rel = np.linalg.norm(da - ga) / np.linalg.norm(ga)
+    print(f"{technique}: |d_albedo - fp64| / |fp64| = {rel:.2e}")
+    assert rel <= 1e-2
+    np.testing.assert_allclose(de, gl, rtol=1e-2)
+
+
+def test_gradient_matches_central_differences(cuda):
+    """Central differences (h = 1e-3) of L = sum (I - T)^2 with common random
+    numbers, for the red wall's albedo (per channel, all its triangles moved
+    together) and for the light's emission. Russian roulette is off here so
+    that the fixed-seed estimator is smooth in the parameters (with it on,
+    the adjoint is the unbiased gradient of the expected image, which
+    per-seed differences do not measure)."""
+    import torch
+    prims = scenes.cornell_box(48, 48)
+    scene, dr = setup(prims, "pt.mis", spp=128, rr_depth=-1)
+    alb0 = triangle_albedo(prims)
+    em0 = light_emission(prims)
+    alb = torch.from_numpy(alb0).to(cuda)
+    em = torch.from_numpy(em0).to(cuda)
+    target = dr.forward(torch.from_numpy((alb0 * 0.8).astype(np.float32)).to(cuda), em * 1.1).double()
+
+    def loss(a, e):
+        return float(((dr.forward(a, e).double() - target) ** 2).sum())
+
+    img = dr.forward(alb, em)
+    da, de = dr.backward(alb, em, 2.0 * (img.double() - target).float())
+    h = 1e-3
+    red = torch.zeros_like(alb)
+    red_tris = np.arange(6, 8)                       # the red wall (primitive 1: triangles 6, 7)
+    for c in range(3):
+        red.zero_()
+        red[red_tris, c] = 1.0
+        fd = (loss(alb + h * red, em) - loss(alb - h * red, em)) / (2 * h)
+        ad = float(da[red_tris, c].sum())
+        print(f"red wall ch{c}: fd {fd:.6e} adjoint {ad:.6e}")
+        assert abs(ad - fd) <= 1e-2 * abs(fd)
+    for c in range(3):
+        e = torch.zeros_like(em)
+        e[0, c] = 1.0
+        fd = (loss(alb, em + h * e) - loss(alb, em - h * e)) / (2 * h)
+        ad = float(de[0, c])
+        print(f"emission ch{c}: fd {fd:.6e} adjoint {ad:.6e}")
+        assert abs(ad - fd) <= 1e-2 * abs(fd)
+
+
+def test_autograd_function(cuda):
+    import torch
+    prims = scenes.cornell_box(32, 32)
+    scene, dr = setup(prims, "pt.mis", spp=16)
+    fn = make_autograd(dr)
+    alb = torch.from_numpy(triangle_albedo(prims)).to(cuda).requires_grad_(True)
+    em = torch.from_numpy(light_emission(prims)).to(cuda).requires_grad_(True)
+    target = dr.forward(alb.detach() * 0.5, em.detach())
+    loss = ((fn(alb, em) - target) ** 2).sum()
+    loss.backward()
+    img = dr.forward(alb.detach(), em.detach())
+    da, de = dr.backward(alb.detach(), em.detach(), 2 * (img - target))
+    torch.testing.assert_close(alb.grad, da, rtol=1e-4, atol=1e-6)
+    torch.testing.assert_close(em.grad, de, rtol=1e-4, atol=1e-6)

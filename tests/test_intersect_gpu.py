@@ -202,3 +202,20 @@ def test_large_scene_layouts_agree(cuda):
     sample = rays[:: (1 << 22) // 20000][:20000]
     o = oracle.OracleScene(pos, faces).intersect(sample)
     np.testing.assert_array_equal(a["tri_id"][:: (1 << 22) // 20000][:20000], o["tri_id"])
+
+
+def test_host_pipeline_matches_device_path(cuda):
+    """lmgpu_intersect_host overlaps copies and traversal of 1M-ray chunks on
+    two streams; each launch must use its own work counter."""
+    import torch
+    pos, faces = random_soup(1 << 18, seed=61, sigma=0.02)
+    rays = random_rays(5 * (1 << 20) + 12345, seed=62)
+    s = gpu_scene(pos, faces, "bvh")
+    for _ in range(3):
+        a = s.intersect_host(rays)
+        soa = {k: torch.from_numpy(v).to(cuda) for k, v in rays_soa(rays).items()}
+        out = torch.empty(rays.shape[0], dtype=torch.int32, device=cuda)
+        s.intersect_device({k: soa[k].data_ptr() for k in soa}, {"tri_id": out.data_ptr()}, rays.shape[0],
+                           torch.cuda.current_stream().cuda_stream)
+        s.status(torch.cuda.current_stream().cuda_stream)
+        np.testing.assert_array_equal(a["tri_id"], out.cpu().numpy())

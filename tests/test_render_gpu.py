@@ -26,7 +26,7 @@ def relmse(x, r):
 
 
 def golden(golden_dir, variant):
-    return np.load(os.path.join(golden_dir, f"cornell_{variant}_ref_mis_4096spp.npz"))["film"]
+    return np.load(os.path.join(golden_dir, f"cornell_{variant}_ref_mis.npz"))["film"]
 
 
 def render(prims, technique, spp, rr_depth=3, max_pv=9, seed=7, sampling="stratified", fp64=False, layout="bvh"):
