@@ -46,6 +46,11 @@ constexpr int32_t STATUS_STACK_OVERFLOW = 1;
 constexpr int32_t STATUS_QUEUE_OVERFLOW = 2;
 constexpr int32_t STATUS_TIMEOUT = 4;
 
+// Path-tracer waves over caller-owned workspace memory (pathtrace.cu).
+int64_t workspace_paths_for_bytes(size_t bytes);
+int render_device_preallocated(LmgpuScene* sc, const LmgpuRenderParams& p, void* film, cudaStream_t stream,
+                               void* ws_mem, size_t ws_bytes, uint32_t* host_counts);
+
 // Frees the path tracer's cached workspace of a scene.
 void release_render_workspace(LmgpuScene* sc);
 

@@ -602,7 +602,88 @@ __global__ void k_rescale(const F* film, float* out, int64_t n, double scale)
     if (i < n) out[i] = (float)((double)film[i] * scale);
 }
 
+// Bytes of wave workspace per path (ensure_workspace's layout) and the
+// fixed header of counters.
+constexpr size_t WS_BYTES_PER_PATH = 16 * 10 + 8 + 4 * 2;
+constexpr size_t WS_HEADER_BYTES = 256;
+
+// Points a Workspace at caller-owned memory (same layout as
+// ensure_workspace, no allocation); host_counts is the caller's readback
+// buffer for the queue counters.
+void carve_workspace(Workspace& ws, void* mem, int64_t paths, uint32_t* host_counts)
+{
+    const size_t P = (size_t)paths;
+    char* p = static_cast<char*>(mem);
+    auto take = [&](size_t b) { char* r = p; p += b; return r; };
+    PathState& st = ws.st;
+    st.counters = reinterpret_cast<uint32_t*>(take(WS_HEADER_BYTES));
+    st.ray_o = reinterpret_cast<float4*>(take(16 * P));
+    st.ray_d = reinterpret_cast<float4*>(take(16 * P));
+    st.hit = reinterpret_cast<float4*>(take(16 * P));
+    st.thr = reinterpret_cast<float4*>(take(16 * P));
+    st.L = reinterpret_cast<float4*>(take(16 * P));
+    st.prev_p = reinterpret_cast<float4*>(take(16 * P));
+    st.prev_n = reinterpret_cast<float4*>(take(16 * P));
+    st.sh_o = reinterpret_cast<float4*>(take(16 * P));
+    st.sh_d = reinterpret_cast<float4*>(take(16 * P));
+    st.sh_c = reinterpret_cast<float4*>(take(16 * P));
+    st.raster = reinterpret_cast<float2*>(take(8 * P));
+    st.queue[0] = reinterpret_cast<int32_t*>(take(4 * P));
+    st.queue[1] = reinterpret_cast<int32_t*>(take(4 * P));
+    ws.mem = mem;
+    ws.capacity = paths;
+    ws.host_counts = host_counts;
+}
+
 }  // namespace
+
+int64_t workspace_paths_for_bytes(size_t bytes)
+{
+    return bytes <= WS_HEADER_BYTES ? 0 : (int64_t)((bytes - WS_HEADER_BYTES) / WS_BYTES_PER_PATH);
+}
+
+// Renders like lmgpu_render_device over a caller-owned wave workspace of
+// `ws_bytes` at `ws_mem` (device) and a host readback buffer of 4 counters:
+// waves never exceed the workspace's capacity, and nothing is allocated.
+int render_device_preallocated(LmgpuScene* sc, const LmgpuRenderParams& p, void* film, cudaStream_t stream,
+                               void* ws_mem, size_t ws_bytes, uint32_t* host_counts)
+{
+    // The same checks as the allocating entry points, without creating the
+    // scene's cached workspace.
+    if (!sc) return fail(LMGPU_ERR_INVALID, "null scene");
+    if (!film) return fail(LMGPU_ERR_INVALID, "null film");
+    if (!sc->dev.cam.valid) return fail(LMGPU_ERR_INVALID, "scene has no camera");
+    if (p.num_samples <= 0) return fail(LMGPU_ERR_INVALID, "num_samples must be positive");
+    if (p.sample_offset < 0) return fail(LMGPU_ERR_INVALID, "negative sample offset");
+    if (p.technique < LMGPU_RENDER_PT || p.technique > LMGPU_RENDER_PT_MIS) return fail(LMGPU_ERR_INVALID, "unknown technique");
+    if (p.sampling != LMGPU_SAMPLING_STRATIFIED && p.sampling != LMGPU_SAMPLING_UNIFORM) return fail(LMGPU_ERR_INVALID, "unknown sampling");
+    if (p.wave_paths < 0) return fail(LMGPU_ERR_INVALID, "negative wave size");
+    int rc = LMGPU_OK;
+    const int64_t cap = workspace_paths_for_bytes(ws_bytes);
+    if (cap <= 0) return fail(LMGPU_ERR_INVALID, "workspace too small");
+    LmgpuRenderParams q = p;
+    q.wave_paths = (int32_t)std::min<int64_t>(p.wave_paths > 0 ? p.wave_paths : cap, cap);
+    Workspace ws;
+    carve_workspace(ws, ws_mem, cap, host_counts);
+    LmgpuRenderStats stats;
+    std::memset(&stats, 0, sizeof(stats));
+    switch (q.technique) {
+    case LMGPU_RENDER_PT:
+        rc = q.film_fp64 ? render_waves<LMGPU_RENDER_PT, double>(sc, q, static_cast<double*>(film), stream, stats, ws)
+                         : render_waves<LMGPU_RENDER_PT, float>(sc, q, static_cast<float*>(film), stream, stats, ws);
+        break;
+    case LMGPU_RENDER_PT_DIRECT:
+        rc = q.film_fp64 ? render_waves<LMGPU_RENDER_PT_DIRECT, double>(sc, q, static_cast<double*>(film), stream, stats, ws)
+                         : render_waves<LMGPU_RENDER_PT_DIRECT, float>(sc, q, static_cast<float*>(film), stream, stats, ws);
+        break;
+    default:
+        rc = q.film_fp64 ? render_waves<LMGPU_RENDER_PT_MIS, double>(sc, q, static_cast<double*>(film), stream, stats, ws)
+                         : render_waves<LMGPU_RENDER_PT_MIS, float>(sc, q, static_cast<float*>(film), stream, stats, ws);
+        break;
+    }
+    if (rc == LMGPU_OK) rc = consume_status(sc, stream);
+    return rc;
+}
 
 // Frees a scene's render workspace (called by lmgpu_scene_destroy).
 void release_render_workspace(LmgpuScene* sc)
