@@ -99,7 +99,10 @@ def test_gradient_matches_central_differences(cuda):
     em0 = light_emission(prims)
     alb = torch.from_numpy(alb0).to(cuda)
     em = torch.from_numpy(em0).to(cuda)
-    target = dr.forward(torch.from_numpy((alb0 * 0.8).astype(np.float32)).to(cuda), em * 1.1).double()
+    # Target with the scene's own emission: pixels that see the light directly
+    # then have I - T ~ 0, so the film's float-atomic summation noise at
+    # those bright pixels (radiance ~17) is not amplified into the loss.
+    target = dr.forward(torch.from_numpy((alb0 * 0.8).astype(np.float32)).to(cuda), em).double()
 
     def loss(a, e):
         return float(((dr.forward(a, e).double() - target) ** 2).sum())
