@@ -2,7 +2,7 @@
 """Benchmark of the B200 scene accelerator / path tracer.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload intersect|render]
+                    [--layout bvh|qbvh] [--sections render,adjoint]
 
 Prints ONE JSON line on rank 0. Multi-GPU runs (torchrun, one process per
 GPU) are independent replicas with weak scaling: every rank traces its own
@@ -14,6 +14,12 @@ uniform on the sphere) against 1,048,576 random triangles (centres U[-1,1]^3,
 edges N(0, 0.01^2)), closest hit with the binary SAH BVH that reproduces the
 reference BVHScene. One step = one launch over the whole ray batch, which is
 larger than L2 (512 MB of rays), so no L2 flush is needed between steps.
+
+At N=1 the same line carries `sections`: the full path tracer at 1920x1080
+(3.4M-triangle terrain + icospheres, 64 spp, pt.mis, max depth 16, RR after
+depth 4) in Mrays/s and spp/s with its relMSE against the reference's FP64
+image, and the adjoint path replay's backward/forward time on the refined
+Cornell box (512x512, 32 spp).
 """
 from __future__ import annotations
 
@@ -50,6 +56,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
     ap.add_argument("--rays-log2", type=int, default=24, help="ray batch 2^k (profiling runs use less)")
+    ap.add_argument("--sections", default="render,adjoint",
+                    help="extra single-GPU sections in the same line: render (1080p path tracer), "
+                         "adjoint (forward/backward cost); '' for none")
     return ap.parse_args()
 
 
@@ -306,6 +315,8 @@ def run_ours(args):
         cpu = {"value": round(rate, 4), "unit": "Mrays/s", "cores": cores, "kind": kind,
                "sample": f"first {done} rays of the 2^24-ray batch ({secs:.1f} s), reference BVHScene built once"}
 
+    sections = run_sections(args, dev, rank, world)
+
     if rank == 0:
         line = {
             "metric": "closest-hit Mrays/s", "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
@@ -327,10 +338,180 @@ def run_ours(args):
             "kernel_ms": {"avg": round(avg_launch_ms, 4), "min": round(min(launch_ms), 4),
                           "max": round(max(launch_ms), 4)},
         }
+        if sections:
+            line["sections"] = sections
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+
+
+# ------------------------------------------------------------- sections ----
+
+TERRAIN_W, TERRAIN_H, TERRAIN_SPP = 1920, 1080, 64
+TERRAIN_RR, TERRAIN_MAX_PV = 5, 17       # Russian roulette after depth 4, max depth 16
+
+
+def _timed_device_renders(L, scene, renderer, num_samples, film, stream, reps, native):
+    """`reps` device renders of `num_samples` samples each (fresh sample
+    ranges), each bracketed by CUDA events on the launching stream."""
+    import torch
+    out = []
+    for k in range(reps):
+        p = renderer.params(num_samples, sample_offset=k * num_samples)
+        st = native.RenderStats()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        native.check(L.lmgpu_render_device(scene.handle, ctypes.byref(p), ctypes.c_void_p(film.data_ptr()),
+                                           ctypes.c_void_p(stream.cuda_stream), ctypes.byref(st)))
+        b.record(stream)
+        torch.cuda.synchronize()
+        out.append((a.elapsed_time(b), st.rays_traced, st.shadow_rays, st.waves))
+    return out
+
+
+def render_section(args, dev, cpu_baseline):
+    """The full path tracer at 1920 x 1080, 64 spp, pt.mis, max depth 16,
+    Russian roulette after depth 4, on the 3.4M-triangle terrain + 64
+    icosphere scene. relMSE is stated against the reference's FP64 pt.mis
+    image of the same scene and camera at 96 x 54 (tests/golden, 16384 spp),
+    rendered here at 65,536 spp."""
+    import torch
+    from lightmetrica_b200 import create_renderer, create_scene, create_scheduler, native, scenes
+    L = native.lib()
+    W, H, S = TERRAIN_W, TERRAIN_H, TERRAIN_SPP
+    t0 = time.perf_counter()
+    prims = scenes.terrain_spheres(W, H)
+    gen_s = time.perf_counter() - t0
+    scene = create_scene(args.layout)
+    scene.load(prims)
+    scene.configure({})
+    scene.build()
+    info = scene.info()
+    r = create_renderer("pt.mis")
+    r.configure({"rr_depth": TERRAIN_RR, "max_path_vertices": TERRAIN_MAX_PV, "sampler": {"rng_seed": 1}})
+    stream = torch.cuda.current_stream(dev)
+    film = torch.zeros(W * H * 3, dtype=torch.float32, device=dev)
+    n = W * H * S
+    _timed_device_renders(L, scene, r, n, film, stream, 1, native)          # warm-up
+    runs = _timed_device_renders(L, scene, r, n, film, stream, 3, native)
+    scene.status(stream.cuda_stream)
+    ms = sum(x[0] for x in runs) / len(runs)
+    rays = sum(x[1] for x in runs) / len(runs)
+    shadow = sum(x[2] for x in runs) / len(runs)
+    # End to end through the scheduler (host film out, rescaled).
+    sched = create_scheduler("mt")
+    sched.configure({"num_samples": n})
+    t0 = time.perf_counter()
+    sched.render(r, scene)
+    e2e_s = time.perf_counter() - t0
+    scene.close()
+
+    # Parity at the scaled-down size against the FP64 reference image.
+    gold = np.load(os.path.join(ROOT, "tests", "golden", "terrain_ref_mis_96x54.npz"))
+    small = scenes.terrain_spheres(96, 54)
+    sc = create_scene(args.layout)
+    sc.load(small)
+    sc.configure({})
+    sc.build()
+    sched = create_scheduler("mt")
+    sched.configure({"num_samples": 96 * 54 * 65536})
+    img = sched.render(r, sc)
+    sc.close()
+    ref = gold["film"].astype(np.float64)
+    rel = float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+    out = {
+        "workload": f"full path tracer: {scenes.num_triangles(prims):,}-triangle fBm heightfield + 64 level-5 "
+                    f"icospheres (diffuse / diffuse-mirror), spherical area light + constant environment 0.5, "
+                    f"{W}x{H}, {S} spp, pt.mis, max depth 16, Russian roulette after depth 4",
+        "Mrays_per_s": round(rays / (ms / 1e3) / 1e6, 1),
+        "spp_per_s": round(S / (ms / 1e3), 2),
+        "Msamples_per_s": round(n / (ms / 1e3) / 1e6, 2),
+        "ms_per_frame": round(ms, 2), "rays_per_frame": int(rays), "shadow_rays_per_frame": int(shadow),
+        "frames_timed": len(runs), "waves_per_frame": runs[0][3],
+        "e2e": {"Mrays_per_s": round(rays / e2e_s / 1e6, 1), "seconds": round(e2e_s, 3),
+                "d2h_bytes_per_step": W * H * 3 * 4, "h2d_bytes_per_step": 0},
+        "relMSE_vs_fp64_reference": rel,
+        "relMSE_case": "96x54 crop-free scale-down, same scene and camera; GPU 65,536 spp vs reference FP64 pt.mis "
+                       f"{int(gold['spp'])} spp",
+        "triangles": scenes.num_triangles(prims), "bvh_nodes": info["num_nodes"],
+        "build_seconds": round(info["build_seconds"], 3), "scene_generation_seconds": round(gen_s, 2),
+    }
+    if cpu_baseline:
+        out["cpu_baseline"] = _render_cpu_baseline(prims, n)
+    return out
+
+
+def _render_cpu_baseline(prims, gpu_samples):
+    """The reference's OpenMP pt.mis (oracle/_ref, float build, `mt`
+    scheduler) on the host cores: a bounded 1-spp sample of the same frame."""
+    try:
+        import oracle
+        if not oracle.ref_available("f"):
+            return {"unavailable": "reference harness not built"}
+        W, H = prims.camera.film.width, prims.camera.film.height
+        threads = os.cpu_count() or 1
+        samples = W * H
+        _, secs = oracle.ref_render(prims, "pt.mis", num_samples=samples, rr_depth=TERRAIN_RR,
+                                    max_path_vertices=TERRAIN_MAX_PV, seed=1, threads=threads, precision="f")
+        return {"Msamples_per_s": round(samples / secs / 1e6, 4), "spp_per_s": round(samples / secs / (W * H), 4),
+                "cores": threads, "kind": "reference",
+                "sample": f"1 spp of the {W}x{H} frame ({samples:,} samples, {secs:.1f} s), BVHScene built untimed"}
+    except Exception as e:      # a reported baseline only; never fails the bench
+        return {"unavailable": str(e)[:200]}
+
+
+def adjoint_section(args, dev):
+    """Adjoint path replay on the Cornell box refined to 34,816 triangles,
+    512 x 512, 32 spp, pt.mis (max depth 8, Russian roulette from depth 3):
+    per-triangle albedo U[0.1, 0.9] (seed 1) against a target rendered with
+    albedos of seed 2. Reports the backward / forward device-time ratio."""
+    import torch
+    from lightmetrica_b200 import create_renderer, create_scene, scenes
+    from lightmetrica_b200.diff import DifferentiableRender, light_emission
+    prims = scenes.cornell_refined(5, 512, 512)
+    scene = create_scene(args.layout)
+    scene.load(prims)
+    scene.configure({})
+    scene.build()
+    r = create_renderer("pt.mis")
+    r.configure({"rr_depth": 3, "max_path_vertices": 9, "sampler": {"rng_seed": 1}})
+    dr = DifferentiableRender(scene, r, 512 * 512 * 32)
+    T = scenes.num_triangles(prims)
+    alb = torch.from_numpy(np.random.default_rng(1).uniform(0.1, 0.9, (T, 3)).astype(np.float32)).to(dev)
+    alb_t = torch.from_numpy(np.random.default_rng(2).uniform(0.1, 0.9, (T, 3)).astype(np.float32)).to(dev)
+    em = torch.from_numpy(light_emission(prims)).to(dev)
+    target = dr.forward(alb_t, em)
+    fwd, bwd = [], []
+    for k in range(4):
+        img = dr.forward(alb, em)
+        f_ms = dr.last_forward_ms
+        dL = 2.0 * (img - target)
+        da, de = dr.backward(alb, em, dL)
+        if k > 0:                       # first pair is warm-up
+            fwd.append(f_ms)
+            bwd.append(dr.last_backward_ms)
+    torch.cuda.synchronize()
+    loss = float(((img - target) ** 2).sum())
+    scene.close()
+    f, b = sum(fwd) / len(fwd), sum(bwd) / len(bwd)
+    return {"workload": f"adjoint path replay: Cornell box refined to {T:,} triangles, 512x512, 32 spp, pt.mis, "
+                        "max depth 8, RR from depth 3; d loss / d (per-triangle albedo, light emission)",
+            "forward_ms": round(f, 3), "backward_ms": round(b, 3), "backward_over_forward": round(b / f, 3),
+            "loss": loss, "grad_norm_albedo": float(da.norm()), "grad_emission": de.cpu().numpy().round(6).tolist()}
+
+
+def run_sections(args, dev, rank, world):
+    names = [x for x in args.sections.split(",") if x]
+    if world > 1 or not names:
+        return None
+    out = {}
+    if "render" in names:
+        out["render_1080p"] = render_section(args, dev, cpu_baseline=(rank == 0 and not args.no_cpu_baseline))
+    if "adjoint" in names:
+        out["adjoint"] = adjoint_section(args, dev)
+    return out
 
 
 def run_e2e(args, scene, rays, hits, world, dev):

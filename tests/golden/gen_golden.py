@@ -20,6 +20,9 @@ Fixtures:
                            the reference's double-precision pt.mis image of
                            lightmetrica_b200.scenes.cornell_box(128, 128,
                            variant) (4096 / 16384 spp)
+  terrain_ref_mis_96x54.npz
+                           the reference's double-precision pt.mis image of
+                           scenes.terrain_spheres at 96 x 54 (16384 spp)
 Each fixture stores the inputs with the reference outputs for every scene
 type the reference builds here (bvh, qbvh, naive).
 """
@@ -151,7 +154,24 @@ def images(variants=("classic", "mixed")):
         print("wrote", variant, "image", f"{spp} spp {secs:.1f} s", film.mean(axis=(0, 1)))
 
 
+def terrain_image(spp: int = 16384):
+    """Image oracle of the full path-tracer scene (scenes.terrain_spheres: a
+    1024 x 1024-vertex fBm heightfield, 64 level-5 icospheres, a spherical
+    area light, a constant environment; 3.4M triangles), scaled down to
+    96 x 54 pixels with the same camera: the reference's double-precision
+    pt.mis, max_path_vertices 17 (max depth 16), rr_depth 5 (Russian roulette
+    after depth 4), at 16384 spp (two independent 4096-spp renders of it
+    differ by relMSE 8.2e-4, so 16384 spp leaves ~1e-4 of noise)."""
+    from lightmetrica_b200 import scenes
+    prims = scenes.terrain_spheres(96, 54)
+    film, secs = oracle.ref_render(prims, "pt.mis", spp=spp, rr_depth=5, max_path_vertices=17, seed=1)
+    np.savez_compressed(os.path.join(OUT, "terrain_ref_mis_96x54.npz"), film=film, spp=spp, rr_depth=5,
+                        max_path_vertices=17, seconds=secs)
+    print("wrote terrain image", f"{spp} spp {secs:.1f} s", film.mean(axis=(0, 1)))
+
+
 if __name__ == "__main__":
     main()
     if oracle.ref_available("d"):
         images()
+        terrain_image()
