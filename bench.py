@@ -56,9 +56,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
     ap.add_argument("--rays-log2", type=int, default=24, help="ray batch 2^k (profiling runs use less)")
-    ap.add_argument("--sections", default="render,adjoint",
+    ap.add_argument("--sections", default="render,adjoint,batch",
                     help="extra single-GPU sections in the same line: render (1080p path tracer), "
-                         "adjoint (forward/backward cost); '' for none")
+                         "adjoint (forward/backward cost), batch (64-scene batch vs plain); '' for none")
     return ap.parse_args()
 
 
@@ -502,6 +502,114 @@ def adjoint_section(args, dev):
             "loss": loss, "grad_norm_albedo": float(da.norm()), "grad_emission": de.cpu().numpy().round(6).tolist()}
 
 
+def batch_section(args, dev):
+    """64 seeded scenes (random-triangle soups and fBm heightfields, 1k-200k
+    triangles, 128^2-1024^2 films, 4-64 spp, max depth 8-16, Lambertian /
+    mirror), pt.mis with Russian roulette after depth 4. Three ways to render
+    the same samples: the batch (one stream of waves over all scenes, each
+    wave a replayed CUDA graph, configuration from the autotuner), the plain
+    one-scene-at-a-time wavefront renderer, and the plain one-scene megakernel
+    (one thread per path, one launch per scene). The batch and the plain
+    renderers trace the same paths, so their relMSE against any reference is
+    equal; the films are compared to show it."""
+    import torch
+    from lightmetrica_b200 import create_renderer, create_scene, native, scenes
+    from lightmetrica_b200.batch import SceneBatch
+    from lightmetrica_b200.diff import DifferentiableRender, light_emission, triangle_albedo
+    L = native.lib()
+    t0 = time.perf_counter()
+    items = [scenes.batch_scene(i) for i in range(64)]
+    built, rs, ns, films = [], [], [], []
+    for i, d in enumerate(items):
+        sc = create_scene("bvh")
+        sc.load(d["prims"])
+        sc.configure({})
+        sc.build()
+        built.append(sc)
+        r = create_renderer("pt.mis")
+        r.configure({"rr_depth": 5, "max_path_vertices": d["max_path_vertices"], "sampler": {"rng_seed": i + 1}})
+        rs.append(r)
+        W = d["prims"].camera.film.width
+        ns.append(W * W * d["spp"])
+        films.append(torch.zeros(W * W * 3, dtype=torch.float32, device=dev))
+    setup_s = time.perf_counter() - t0
+    stream = torch.cuda.current_stream(dev)
+    total = sum(ns)
+
+    def zero():
+        for f in films:
+            f.zero_()
+
+    def plain_pass():
+        st = native.RenderStats()
+        rays = 0
+        for sc, r, n, f in zip(built, rs, ns, films):
+            p = r.params(n)
+            native.check(L.lmgpu_render_device(sc.handle, ctypes.byref(p), ctypes.c_void_p(f.data_ptr()),
+                                               ctypes.c_void_p(stream.cuda_stream), ctypes.byref(st)))
+            rays += st.rays_traced
+        return rays
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        out = fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b), out
+
+    # Plain wavefront, one scene at a time.
+    zero()
+    plain_pass()                                          # warm-up
+    zero()
+    plain_ms, plain_rays = timed(plain_pass)
+    plain = [f.clone() for f in films]
+
+    # Plain megakernel, one launch per scene (scene's own albedo and emission).
+    drs = [DifferentiableRender(sc, r, n) for sc, r, n in zip(built, rs, ns)]
+    params = [(torch.from_numpy(triangle_albedo(d["prims"])).to(dev), torch.from_numpy(light_emission(d["prims"])).to(dev))
+              for d in items]
+
+    def mega_pass():
+        return [dr.forward(a, e) for dr, (a, e) in zip(drs, params)]
+    mega_pass()
+    mega_ms, _ = timed(mega_pass)
+
+    # Batch: autotune (untimed, like a build step), warm-up, timed render.
+    batch = SceneBatch(built)
+    t0 = time.perf_counter()
+    tuned = batch.autotune(rs, ns, sample_fraction=1.0 / 16)
+    tune_s = time.perf_counter() - t0
+    zero()
+    batch.render_device(rs, ns, films)
+    zero()
+    batch_ms, _ = timed(lambda: batch.render_device(rs, ns, films, stats=False))
+    batch.render_device(rs, ns, [torch.zeros_like(f) for f in films])     # stats of one render
+    st = batch.last_stats
+    rel = []
+    for a, b in zip(films, plain):
+        a64, b64 = a.double(), b.double()
+        rel.append(float(((a64 - b64) ** 2 / (b64 ** 2 + 1e-2)).mean()))
+    batch.close()
+    for sc in built:
+        sc.close()
+    return {"workload": "64 scenes (soups / heightfields, log-uniform 1k-200k triangles, 128^2-1024^2, 4-64 spp, "
+                        "max depth 8-16, Lambertian / mirror), pt.mis, RR after depth 4",
+            "samples": total, "triangles": sum(d["triangles"] for d in items),
+            "batched_ms": round(batch_ms, 2), "plain_wavefront_ms": round(plain_ms, 2),
+            "plain_megakernel_ms": round(mega_ms, 2),
+            "batched_over_plain_wavefront": round(plain_ms / batch_ms, 3),
+            "batched_over_plain_megakernel": round(mega_ms / batch_ms, 3),
+            "batched_Mrays_per_s": round(st["rays_traced"] / (batch_ms / 1e3) / 1e6, 1),
+            "batched_Msamples_per_s": round(total / (batch_ms / 1e3) / 1e6, 1),
+            "plain_wavefront_Mrays_per_s": round(plain_rays / (plain_ms / 1e3) / 1e6, 1),
+            "waves": st["waves"], "autotuned": tuned, "autotune_seconds": round(tune_s, 2),
+            "setup_seconds": round(setup_s, 2),
+            "relMSE_batched_vs_plain_max": max(rel),
+            "equal_relMSE": "same samples and paths in both; films differ only by float-atomic summation order"}
+
+
 def run_sections(args, dev, rank, world):
     names = [x for x in args.sections.split(",") if x]
     if world > 1 or not names:
@@ -511,6 +619,8 @@ def run_sections(args, dev, rank, world):
         out["render_1080p"] = render_section(args, dev, cpu_baseline=(rank == 0 and not args.no_cpu_baseline))
     if "adjoint" in names:
         out["adjoint"] = adjoint_section(args, dev)
+    if "batch" in names:
+        out["batch64"] = batch_section(args, dev)
     return out
 
 

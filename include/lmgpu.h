@@ -268,6 +268,50 @@ int lmgpu_adjoint_backward(LmgpuScene* scene, const LmgpuRenderParams* params,
                            float* d_albedo_device, float* d_emission_device,
                            void* stream, LmgpuRenderStats* stats);
 
+/* ------------------------------------------------ multi-scene batch ---- */
+/* No counterpart in the reference (its schedulers render one scene at a
+ * time, sched.mt.cpp:93-266). A batch renders many independent scenes, each
+ * with its own camera, film and render parameters, as one stream of waves:
+ * a wave's paths span several scenes and every path carries its scene
+ * index, so small scenes share the GPU instead of running one after the
+ * other. Each wave (initialisation, every bounce, splat) is captured once
+ * into a CUDA graph and replayed per wave with no host synchronisation in
+ * between. Every scene renders exactly the samples it would render alone
+ * with the same parameters (same random numbers, same paths). */
+typedef struct LmgpuBatch LmgpuBatch;
+
+typedef struct LmgpuBatchConfig {
+    int32_t layout;               /* LMGPU_LAYOUT_BVH2 or LMGPU_LAYOUT_BVH4 for every scene */
+    int32_t wave_paths;           /* paths per wave: the capacity of the ray and shadow queues */
+    int32_t shade_blocks_per_sm;  /* grid of the shading kernel (blocks of 128 threads per SM) */
+    int32_t use_graph;            /* 1: waves replay a captured CUDA graph; 0: direct launches */
+} LmgpuBatchConfig;
+
+/* The scenes (built with a BVH layout, on the current device) must outlive
+ * the batch; a scene may appear more than once. Default configuration:
+ * BVH2, 2^21 paths per wave, 8 shading blocks per SM, graphs on. */
+int lmgpu_batch_create(LmgpuScene* const* scenes, int32_t num_scenes, LmgpuBatch** out);
+int lmgpu_batch_destroy(LmgpuBatch* batch);
+int lmgpu_batch_get_config(const LmgpuBatch* batch, LmgpuBatchConfig* config);
+int lmgpu_batch_set_config(LmgpuBatch* batch, const LmgpuBatchConfig* config);
+
+/* Renders every scene of the batch: params[i] and films_device[i] belong to
+ * scene i, with lmgpu_render_device's meaning (un-rescaled DEVICE film, float
+ * or double by film_fp64; the caller zeroes it). All params share one
+ * technique and one film type; wave_paths is ignored (the batch's
+ * configuration sets it). Asynchronous on `stream` unless `stats` is given,
+ * in which case the call synchronises and fills the totals of the batch. */
+int lmgpu_batch_render_device(LmgpuBatch* batch, const LmgpuRenderParams* params,
+                              void* const* films_device, void* stream, LmgpuRenderStats* stats);
+
+/* Autotuner: renders the batch with each scene's sample count scaled by
+ * `sample_fraction` (0 < f <= 1) under candidate configurations (BVH
+ * layout, wave size, shading grid), coordinate by coordinate, keeps the
+ * fastest, stores it as the batch's configuration and returns it with its
+ * device time in ms. Films are scratch memory of the tuner; synchronises. */
+int lmgpu_batch_autotune(LmgpuBatch* batch, const LmgpuRenderParams* params, double sample_fraction,
+                         void* stream, LmgpuBatchConfig* chosen, double* best_ms);
+
 /* ------------------------------------------------------------- misc ----- */
 const char* lmgpu_last_error(void);
 int lmgpu_abi_version(void);

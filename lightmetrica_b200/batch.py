@@ -1,0 +1,136 @@
+"""Multi-scene batch rendering through lmgpu_batch_* (no counterpart in the
+reference, whose RenderProcessScheduler renders one scene at a time,
+sched.mt.cpp:93-266).
+
+    batch = SceneBatch([scene_a, scene_b, ...])       # built Scene objects
+    batch.autotune(renderers, num_samples)            # optional: layout, wave size, shading grid
+    films = batch.render(renderers, num_samples)      # one (H, W, 3) film per scene
+
+Each scene keeps its own camera, film, renderer parameters (technique shared
+by the batch) and sample count, and renders exactly the samples it would
+render alone through RenderProcessScheduler.render: same random numbers,
+same paths. All scenes' paths run in shared waves whose kernel sequence is
+replayed from a captured CUDA graph.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Sequence
+
+import numpy as np
+
+from . import native as N
+from .render import Renderer
+
+LAYOUTS = {"bvh": N.LAYOUT_BVH2, "qbvh": N.LAYOUT_BVH4}
+
+
+class SceneBatch:
+    def __init__(self, scenes: Sequence):
+        if not scenes:
+            raise ValueError("a batch needs at least one scene")
+        self.scenes = list(scenes)
+        arr = (ctypes.c_void_p * len(self.scenes))(*[s.handle.value for s in self.scenes])
+        self._keep = arr
+        self.handle = ctypes.c_void_p()
+        N.check(N.lib().lmgpu_batch_create(arr, len(self.scenes), ctypes.byref(self.handle)))
+        self.last_stats = None
+
+    # ------------------------------------------------------------ config --
+    @property
+    def config(self) -> dict:
+        c = N.BatchConfig()
+        N.check(N.lib().lmgpu_batch_get_config(self.handle, ctypes.byref(c)))
+        return {"layout": {v: k for k, v in LAYOUTS.items()}[c.layout], "wave_paths": c.wave_paths,
+                "shade_blocks_per_sm": c.shade_blocks_per_sm, "use_graph": bool(c.use_graph)}
+
+    def configure(self, layout: str | None = None, wave_paths: int | None = None,
+                  shade_blocks_per_sm: int | None = None, use_graph: bool | None = None) -> None:
+        c = N.BatchConfig()
+        N.check(N.lib().lmgpu_batch_get_config(self.handle, ctypes.byref(c)))
+        if layout is not None:
+            if layout not in LAYOUTS:
+                raise ValueError("layout must be 'bvh' or 'qbvh'")
+            c.layout = LAYOUTS[layout]
+        if wave_paths is not None:
+            c.wave_paths = int(wave_paths)
+        if shade_blocks_per_sm is not None:
+            c.shade_blocks_per_sm = int(shade_blocks_per_sm)
+        if use_graph is not None:
+            c.use_graph = 1 if use_graph else 0
+        N.check(N.lib().lmgpu_batch_set_config(self.handle, ctypes.byref(c)))
+
+    # ------------------------------------------------------------ render --
+    def _params(self, renderers, num_samples, film_fp64):
+        n = len(self.scenes)
+        if isinstance(renderers, Renderer):
+            renderers = [renderers] * n
+        if np.isscalar(num_samples):
+            num_samples = [int(num_samples)] * n
+        if len(renderers) != n or len(num_samples) != n:
+            raise ValueError("one renderer and one sample count per scene")
+        arr = (N.RenderParams * n)()
+        for i, (r, k) in enumerate(zip(renderers, num_samples)):
+            arr[i] = r.params(int(k), film_fp64=film_fp64)
+        return arr
+
+    def render_device(self, renderers, num_samples, films, stream=None, stats: bool = True):
+        """Accumulates each scene's un-rescaled samples into `films[i]`
+        (CUDA tensors of W*H*3 float32, or float64 with film_fp64)."""
+        import torch
+        fp64 = films[0].dtype == torch.float64
+        params = self._params(renderers, num_samples, fp64)
+        ptrs = (ctypes.c_void_p * len(films))(*[f.data_ptr() for f in films])
+        s = stream if stream is not None else torch.cuda.current_stream(films[0].device).cuda_stream
+        st = N.RenderStats() if stats else None
+        N.check(N.lib().lmgpu_batch_render_device(self.handle, params, ptrs, ctypes.c_void_p(s),
+                                                  ctypes.byref(st) if stats else None))
+        if stats:
+            self.last_stats = {"rays_traced": st.rays_traced, "shadow_rays": st.shadow_rays, "paths": st.paths,
+                               "waves": st.waves, "max_bounces_run": st.max_bounces_run, "device_ms": st.device_ms}
+        return films
+
+    def render(self, renderers, num_samples, film_fp64: bool = False):
+        """Renders every scene; returns the rescaled films (H, W, 3) as numpy
+        arrays (the reference's Rescale(W * H / num_samples))."""
+        import torch
+        n = len(self.scenes)
+        if np.isscalar(num_samples):
+            num_samples = [int(num_samples)] * n
+        dt = torch.float64 if film_fp64 else torch.float32
+        films = []
+        for s in self.scenes:
+            cam = s.main_camera()
+            films.append(torch.zeros(cam.film.width * cam.film.height * 3, dtype=dt, device="cuda"))
+        self.render_device(renderers, num_samples, films)
+        out = []
+        for s, f, k in zip(self.scenes, films, num_samples):
+            cam = s.main_camera()
+            W, H = cam.film.width, cam.film.height
+            out.append((f.double() * (W * H / k)).float().cpu().numpy().reshape(H, W, 3))
+        return out
+
+    def autotune(self, renderers, num_samples, sample_fraction: float = 0.125, stream=None) -> dict:
+        """Chooses layout, wave size and shading grid by timing scaled-down
+        renders of this batch; the choice becomes the batch's configuration."""
+        import torch
+        params = self._params(renderers, num_samples, False)
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        c = N.BatchConfig()
+        ms = ctypes.c_double()
+        N.check(N.lib().lmgpu_batch_autotune(self.handle, params, float(sample_fraction), ctypes.c_void_p(s),
+                                             ctypes.byref(c), ctypes.byref(ms)))
+        out = self.config
+        out["trial_ms"] = ms.value
+        return out
+
+    def close(self) -> None:
+        if self.handle is not None and self.handle.value:
+            N.lib().lmgpu_batch_destroy(self.handle)
+        self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

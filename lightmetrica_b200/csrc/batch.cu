@@ -1,0 +1,614 @@
+// Multi-scene batch: many independent scenes rendered as one stream of
+// waves, each wave captured once into a CUDA graph and replayed.
+//
+// The one-scene driver (pathtrace.cu) reads every queue count back to the
+// host to size its next launch, so a small scene spends most of its time in
+// launch gaps and host round trips, and the GPU renders one scene at a time.
+// Here the waves run over the concatenated sample sequence of all scenes
+// (SceneTable context: per-path scene index, per-ray scene in traversal),
+// launches have fixed grids that read their counts on the device, and one
+// wave (init, K bounces of trace / shade / shadow, splat, wave advance) is a
+// fixed kernel sequence: captured into a graph once per configuration and
+// launched once per wave with no host synchronisation. Scenes whose depth is
+// unbounded (max_path_vertices = -1) finish their tail bounces with direct
+// launches after the graph.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../../include/lmgpu.h"
+#include "internal.h"
+#include "pt_kernels.cuh"
+#include "trace_kernels.cuh"
+
+using namespace lmgpu;
+
+namespace {
+
+constexpr int WORK_SLOTS = 160;            // traversal launches per wave: 2 per bounce + 1
+constexpr int GRAPH_BOUNCES_UNBOUNDED = 24;
+constexpr int MAX_BOUNDED_BOUNCES = 64;
+constexpr size_t BYTES_PER_PATH = 16 * 10 + 8 + 4 * 2 + 4;   // path state + scene index
+
+// Device totals of a render: [0] closest-hit rays, [1] shadow rays,
+// [2] deepest bounce with a live ray.
+constexpr int NSTATS = 4;
+
+struct GraphKey {
+    int tech = -1, fp64 = -1, layout = -1, stack = -1, bounces = -1, bounded = -1, shade_blocks = -1;
+    int64_t paths = -1;
+    int num_scenes = -1;
+    bool operator==(const GraphKey& o) const
+    {
+        return tech == o.tech && fp64 == o.fp64 && layout == o.layout && stack == o.stack && bounces == o.bounces &&
+               bounded == o.bounded && shade_blocks == o.shade_blocks && paths == o.paths && num_scenes == o.num_scenes;
+    }
+};
+
+}  // namespace
+
+struct LmgpuBatch {
+    int device = 0;
+    int sms = 148;
+    std::vector<LmgpuScene*> scenes;
+    LmgpuBatchConfig cfg{ LMGPU_LAYOUT_BVH2, 1 << 21, 8, 1 };
+
+    BatchEntry* d_table = nullptr;
+    int64_t* d_begins = nullptr;
+    WaveCtl* d_wave = nullptr;
+    unsigned long long* d_stats = nullptr;
+    unsigned long long* d_work = nullptr;
+    int32_t* d_status = nullptr;
+    BatchEntry* h_table = nullptr;          // pinned staging
+    int64_t* h_begins = nullptr;
+    unsigned long long* h_stats = nullptr;
+    uint32_t* h_counts = nullptr;
+    cudaEvent_t staged = nullptr;           // the staging buffers' last copy has run
+
+    void* ws_mem = nullptr;
+    int64_t ws_capacity = 0;
+    PathState st{};
+
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    GraphKey key;
+};
+
+namespace {
+
+// ------------------------------------------------------ small kernels ----
+
+__global__ void k_batch_setup(WaveCtl* wave, int64_t total, int64_t step, unsigned long long* stats)
+{
+    wave->base = 0;
+    wave->count = step < total ? step : total;
+    wave->total = total;
+    wave->step = step;
+    for (int i = 0; i < NSTATS; i++) stats[i] = 0;
+}
+
+// Start of a wave: clear the queue counters and this wave's traversal work
+// counters.
+__global__ void k_wave_begin(uint32_t* counters, unsigned long long* work, int slots)
+{
+    for (int i = threadIdx.x; i < slots; i += blockDim.x) work[i] = 0;
+    if (threadIdx.x < 4) counters[threadIdx.x] = 0;
+}
+
+// Before bounce k: tally the rays about to be traced and the shadow rays of
+// the previous pass, then clear the output queue and the shadow queue.
+__global__ void k_bounce_prep(uint32_t* counters, int qin, int k, unsigned long long* stats)
+{
+    const uint32_t n = counters[qin];
+    stats[0] += n;
+    stats[1] += counters[2];
+    if (n > 0 && (unsigned long long)k > stats[2]) stats[2] = (unsigned long long)k;
+    counters[1 - qin] = 0;
+    counters[2] = 0;
+}
+
+// End of a wave (after the splat): last shadow tally, advance to the next wave.
+__global__ void k_wave_end(WaveCtl* wave, uint32_t* counters, unsigned long long* stats)
+{
+    stats[1] += counters[2];
+    counters[2] = 0;
+    const int64_t base = wave->base + wave->step;
+    wave->base = base;
+    const int64_t left = wave->total - base;
+    wave->count = left <= 0 ? 0 : (left < wave->step ? left : wave->step);
+}
+
+// ------------------------------------------------------- wave builder ----
+
+struct Launch {
+    int64_t paths;             // wave capacity
+    int shade_blocks;
+    int trace_blocks;          // closest-hit grid
+    int shadow_blocks;         // any-hit grid
+    DeviceScene proto;         // template scene for the traversal kernel (layout only)
+};
+
+template <int TECH, class F, int LAYOUT, int STACK>
+struct Wave {
+    using Ctx = SceneTable<float>;     // init / shade use no film
+    using FilmCtx = SceneTable<F>;
+
+    static Ctx ctx(const LmgpuBatch* b) { return Ctx{ b->d_table, b->d_begins, (int32_t)b->scenes.size(), b->d_wave }; }
+    static FilmCtx film_ctx(const LmgpuBatch* b)
+    {
+        return FilmCtx{ b->d_table, b->d_begins, (int32_t)b->scenes.size(), b->d_wave };
+    }
+
+    static void shadow(const LmgpuBatch* b, const Launch& L, int slot, cudaStream_t s)
+    {
+        const PathState& st = b->st;
+        ShadowIO<FilmCtx> io{ st.counters + 2, st.sh_o, st.sh_d, st.sh_c, st.L, film_ctx(b) };
+        k_trace_persistent<LAYOUT, STACK, true, ShadowIO<FilmCtx>><<<L.shadow_blocks, 128, 0, s>>>(
+            L.proto, io, b->d_status, b->d_work + slot);
+    }
+
+    static void bounce(const LmgpuBatch* b, const Launch& L, int k, int qin, int slot, cudaStream_t s)
+    {
+        const PathState& st = b->st;
+        k_bounce_prep<<<1, 1, 0, s>>>(st.counters, qin, k, b->d_stats);
+        PathRayIO<true> io{ st.queue[qin], st.counters + qin, st.ray_o, st.ray_d, st.hit, b->d_table, st.scene };
+        k_trace_persistent<LAYOUT, STACK, false, PathRayIO<true>><<<L.trace_blocks, 128, 0, s>>>(
+            L.proto, io, b->d_status, b->d_work + slot);
+        k_pt_shade<TECH, Ctx><<<L.shade_blocks, 128, 0, s>>>(ctx(b), st, k, qin, 1 - qin);
+        if (TECH != LMGPU_RENDER_PT) shadow(b, L, slot + 1, s);
+    }
+
+    // init + bounces 1..K (+ splat and wave advance when `finish`).
+    static void body(const LmgpuBatch* b, const Launch& L, int K, bool finish, cudaStream_t s)
+    {
+        const PathState& st = b->st;
+        k_wave_begin<<<1, 128, 0, s>>>(st.counters, b->d_work, WORK_SLOTS);
+        k_pt_init<TECH, Ctx><<<(unsigned)((L.paths + 127) / 128), 128, 0, s>>>(ctx(b), st, 0);
+        int slot = 0;
+        if (TECH != LMGPU_RENDER_PT) shadow(b, L, slot++, s);
+        for (int k = 1; k <= K; k++, slot += 2) bounce(b, L, k, (k - 1) & 1, slot, s);
+        if (finish) tail_end(b, L, s);
+    }
+
+    static void tail_end(const LmgpuBatch* b, const Launch& L, cudaStream_t s)
+    {
+        k_pt_splat<FilmCtx><<<(unsigned)((L.paths + 127) / 128), 128, 0, s>>>(film_ctx(b), b->st, 0);
+        k_wave_end<<<1, 1, 0, s>>>(b->d_wave, b->st.counters, b->d_stats);
+    }
+
+    static void warm(Launch& L)
+    {
+        L.trace_blocks = resident_blocks(k_trace_persistent<LAYOUT, STACK, false, PathRayIO<true>>);
+        L.shadow_blocks = resident_blocks(k_trace_persistent<LAYOUT, STACK, true, ShadowIO<FilmCtx>>);
+    }
+};
+
+// ------------------------------------------------------------ driver ------
+
+int ensure_batch_workspace(LmgpuBatch* b, int64_t paths)
+{
+    if (b->ws_capacity >= paths && b->ws_mem) return LMGPU_OK;
+    if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; b->key = GraphKey{}; }
+    if (b->ws_mem) { cudaFree(b->ws_mem); b->ws_mem = nullptr; b->ws_capacity = 0; }
+    const size_t P = (size_t)paths;
+    cudaError_t e = cudaMalloc(&b->ws_mem, P * BYTES_PER_PATH + 256);
+    if (e != cudaSuccess) {
+        b->ws_mem = nullptr;
+        return e == cudaErrorMemoryAllocation ? fail(LMGPU_ERR_OOM, "batch workspace allocation failed")
+                                              : cuda_fail(e, "cudaMalloc(batch workspace)");
+    }
+    char* p = static_cast<char*>(b->ws_mem);
+    auto take = [&](size_t n) { char* r = p; p += n; return r; };
+    PathState& st = b->st;
+    st.counters = reinterpret_cast<uint32_t*>(take(256));
+    st.ray_o = reinterpret_cast<float4*>(take(16 * P));
+    st.ray_d = reinterpret_cast<float4*>(take(16 * P));
+    st.hit = reinterpret_cast<float4*>(take(16 * P));
+    st.thr = reinterpret_cast<float4*>(take(16 * P));
+    st.L = reinterpret_cast<float4*>(take(16 * P));
+    st.prev_p = reinterpret_cast<float4*>(take(16 * P));
+    st.prev_n = reinterpret_cast<float4*>(take(16 * P));
+    st.sh_o = reinterpret_cast<float4*>(take(16 * P));
+    st.sh_d = reinterpret_cast<float4*>(take(16 * P));
+    st.sh_c = reinterpret_cast<float4*>(take(16 * P));
+    st.raster = reinterpret_cast<float2*>(take(8 * P));
+    st.queue[0] = reinterpret_cast<int32_t*>(take(4 * P));
+    st.queue[1] = reinterpret_cast<int32_t*>(take(4 * P));
+    st.scene = reinterpret_cast<int32_t*>(take(4 * P));
+    b->ws_capacity = paths;
+    return LMGPU_OK;
+}
+
+int consume_batch_status(LmgpuBatch* b, cudaStream_t s)
+{
+    int32_t v = 0;
+    LMGPU_CUDA_TRY(cudaMemcpyAsync(&v, b->d_status, sizeof(v), cudaMemcpyDeviceToHost, s));
+    LMGPU_CUDA_TRY(cudaStreamSynchronize(s));
+    if (v == 0) return LMGPU_OK;
+    LMGPU_CUDA_TRY(cudaMemsetAsync(b->d_status, 0, sizeof(int32_t), s));
+    if (v & STATUS_STACK_OVERFLOW) return fail(LMGPU_ERR_STACK_OVERFLOW, "traversal stack bound exceeded");
+    return fail(LMGPU_ERR_CUDA, "unknown device status");
+}
+
+// Everything a render needs to know about its parameters.
+struct Plan {
+    int tech, fp64, stack, bounces;
+    bool bounded;
+    int64_t total;
+};
+
+int make_plan(LmgpuBatch* b, const LmgpuRenderParams* params, void* const* films, Plan& pl)
+{
+    const int n = (int)b->scenes.size();
+    if (!params) return fail(LMGPU_ERR_INVALID, "null params");
+    pl.tech = params[0].technique;
+    pl.fp64 = params[0].film_fp64 ? 1 : 0;
+    pl.total = 0;
+    pl.bounded = true;
+    int max_pv = 1, cap = 0;
+    for (int i = 0; i < n; i++) {
+        const LmgpuRenderParams& p = params[i];
+        const LmgpuScene* sc = b->scenes[i];
+        if (films && !films[i]) return fail(LMGPU_ERR_INVALID, "null film");
+        if (p.technique != pl.tech) return fail(LMGPU_ERR_INVALID, "a batch renders with one technique");
+        if ((p.film_fp64 ? 1 : 0) != pl.fp64) return fail(LMGPU_ERR_INVALID, "a batch uses one film type");
+        if (p.technique < LMGPU_RENDER_PT || p.technique > LMGPU_RENDER_PT_MIS) return fail(LMGPU_ERR_INVALID, "unknown technique");
+        if (p.sampling != LMGPU_SAMPLING_STRATIFIED && p.sampling != LMGPU_SAMPLING_UNIFORM) return fail(LMGPU_ERR_INVALID, "unknown sampling");
+        if (p.num_samples <= 0) return fail(LMGPU_ERR_INVALID, "num_samples must be positive");
+        if (p.sample_offset < 0) return fail(LMGPU_ERR_INVALID, "negative sample offset");
+        if (!sc->dev.cam.valid) return fail(LMGPU_ERR_INVALID, "scene has no camera");
+        pl.total += p.num_samples;
+        if (p.max_path_vertices == -1) pl.bounded = false;
+        else max_pv = std::max(max_pv, p.max_path_vertices);
+        cap = std::max(cap, sc->dev.stack_cap);
+    }
+    if (pl.total >= (int64_t(1) << 62)) return fail(LMGPU_ERR_INVALID, "sample count too large");
+    pl.bounces = pl.bounded ? max_pv - 1 : GRAPH_BOUNCES_UNBOUNDED;
+    if (pl.bounded && pl.bounces > MAX_BOUNDED_BOUNCES) {
+        pl.bounded = false;
+        pl.bounces = GRAPH_BOUNCES_UNBOUNDED;
+    }
+    if (cap <= 64) pl.stack = 64;
+    else if (cap <= 128) pl.stack = 128;
+    else if (cap <= 256) pl.stack = 256;
+    else return fail(LMGPU_ERR_UNSUPPORTED, "BVH deeper than the largest compiled traversal stack (256)");
+    return LMGPU_OK;
+}
+
+int upload_table(LmgpuBatch* b, const LmgpuRenderParams* params, void* const* films, cudaStream_t s)
+{
+    const int n = (int)b->scenes.size();
+    // The previous call's copies read the same pinned buffers.
+    LMGPU_CUDA_TRY(cudaEventSynchronize(b->staged));
+    int64_t begin = 0;
+    for (int i = 0; i < n; i++) {
+        const LmgpuRenderParams& p = params[i];
+        BatchEntry& e = b->h_table[i];
+        e.s = b->scenes[i]->dev;
+        e.s.layout = b->cfg.layout;
+        e.rc.technique = p.technique;
+        e.rc.rr_depth = p.rr_depth;
+        e.rc.max_pv = p.max_path_vertices;
+        e.rc.sampling = p.sampling;
+        e.rc.seed = p.seed;
+        e.rc.sample_base = p.sample_offset;
+        e.rc.pixels = (int64_t)e.s.cam.width * e.s.cam.height;
+        e.begin = begin;
+        e.film = films[i];
+        b->h_begins[i] = begin;
+        begin += p.num_samples;
+    }
+    b->h_begins[n] = begin;
+    LMGPU_CUDA_TRY(cudaMemcpyAsync(b->d_table, b->h_table, n * sizeof(BatchEntry), cudaMemcpyHostToDevice, s));
+    LMGPU_CUDA_TRY(cudaMemcpyAsync(b->d_begins, b->h_begins, (n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    LMGPU_CUDA_TRY(cudaEventRecord(b->staged, s));
+    return LMGPU_OK;
+}
+
+template <int TECH, class F, int LAYOUT, int STACK>
+int run_waves(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_t& waves)
+{
+    using W = Wave<TECH, F, LAYOUT, STACK>;
+    Launch L;
+    L.paths = P;
+    L.shade_blocks = std::max(1, b->cfg.shade_blocks_per_sm) * b->sms;
+    L.proto = b->scenes[0]->dev;
+    L.proto.layout = LAYOUT;
+    W::warm(L);
+    waves = (pl.total + P - 1) / P;
+    k_batch_setup<<<1, 1, 0, s>>>(b->d_wave, pl.total, P, b->d_stats);
+    LMGPU_CUDA_TRY(cudaGetLastError());
+
+    if (b->cfg.use_graph) {
+        GraphKey key;
+        key.tech = TECH; key.fp64 = pl.fp64; key.layout = LAYOUT; key.stack = STACK; key.bounces = pl.bounces;
+        key.bounded = pl.bounded; key.shade_blocks = L.shade_blocks; key.paths = P; key.num_scenes = (int)b->scenes.size();
+        if (!b->exec || !(b->key == key)) {
+            if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; b->key = GraphKey{}; }
+            LMGPU_CUDA_TRY(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
+            W::body(b, L, pl.bounces, pl.bounded, b->cap_stream);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(b->cap_stream, &g);
+            if (e != cudaSuccess) return cuda_fail(e, "graph capture of a batch wave");
+            e = cudaGraphInstantiate(&b->exec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) { b->exec = nullptr; return cuda_fail(e, "cudaGraphInstantiate"); }
+            b->key = key;
+        }
+    }
+    for (int64_t w = 0; w < waves; w++) {
+        if (b->cfg.use_graph) LMGPU_CUDA_TRY(cudaGraphLaunch(b->exec, s));
+        else W::body(b, L, pl.bounces, pl.bounded, s);
+        LMGPU_CUDA_TRY(cudaGetLastError());
+        if (pl.bounded) continue;
+        // Unbounded depth: finish the wave's remaining bounces directly.
+        int k = pl.bounces + 1;
+        int slot = (TECH != LMGPU_RENDER_PT ? 1 : 0);   // counters reused: clear before each launch
+        for (;; k++) {
+            const int qin = (k - 1) & 1;
+            LMGPU_CUDA_TRY(cudaMemcpyAsync(b->h_counts, b->st.counters, 16, cudaMemcpyDeviceToHost, s));
+            LMGPU_CUDA_TRY(cudaStreamSynchronize(s));
+            if (b->h_counts[qin] == 0) break;
+            LMGPU_CUDA_TRY(cudaMemsetAsync(b->d_work + slot, 0, 2 * sizeof(unsigned long long), s));
+            W::bounce(b, L, k, qin, slot, s);
+            LMGPU_CUDA_TRY(cudaGetLastError());
+        }
+        W::tail_end(b, L, s);
+        LMGPU_CUDA_TRY(cudaGetLastError());
+    }
+    return LMGPU_OK;
+}
+
+template <int TECH, class F>
+int dispatch_layout(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_t& waves)
+{
+    const bool bvh4 = b->cfg.layout == LMGPU_LAYOUT_BVH4;
+    switch (pl.stack) {
+    case 64: return bvh4 ? run_waves<TECH, F, LMGPU_LAYOUT_BVH4, 64>(b, pl, P, s, waves)
+                         : run_waves<TECH, F, LMGPU_LAYOUT_BVH2, 64>(b, pl, P, s, waves);
+    case 128: return bvh4 ? run_waves<TECH, F, LMGPU_LAYOUT_BVH4, 128>(b, pl, P, s, waves)
+                          : run_waves<TECH, F, LMGPU_LAYOUT_BVH2, 128>(b, pl, P, s, waves);
+    default: return bvh4 ? run_waves<TECH, F, LMGPU_LAYOUT_BVH4, 256>(b, pl, P, s, waves)
+                         : run_waves<TECH, F, LMGPU_LAYOUT_BVH2, 256>(b, pl, P, s, waves);
+    }
+}
+
+template <class F>
+int dispatch_tech(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_t& waves)
+{
+    switch (pl.tech) {
+    case LMGPU_RENDER_PT: return dispatch_layout<LMGPU_RENDER_PT, F>(b, pl, P, s, waves);
+    case LMGPU_RENDER_PT_DIRECT: return dispatch_layout<LMGPU_RENDER_PT_DIRECT, F>(b, pl, P, s, waves);
+    default: return dispatch_layout<LMGPU_RENDER_PT_MIS, F>(b, pl, P, s, waves);
+    }
+}
+
+int check_config(const LmgpuBatchConfig& c)
+{
+    if (c.layout != LMGPU_LAYOUT_BVH2 && c.layout != LMGPU_LAYOUT_BVH4)
+        return fail(LMGPU_ERR_INVALID, "batch layout must be LMGPU_LAYOUT_BVH2 or LMGPU_LAYOUT_BVH4");
+    if (c.wave_paths < 1024 || c.wave_paths > (1 << 24)) return fail(LMGPU_ERR_INVALID, "wave_paths must be in [1024, 2^24]");
+    if (c.shade_blocks_per_sm < 1 || c.shade_blocks_per_sm > 64) return fail(LMGPU_ERR_INVALID, "shade_blocks_per_sm must be in [1, 64]");
+    return LMGPU_OK;
+}
+
+// Renders with the batch's current configuration; device time in *ms when
+// `ms` is given (synchronises).
+int batch_render(LmgpuBatch* b, const LmgpuRenderParams* params, void* const* films, cudaStream_t s,
+                 LmgpuRenderStats* stats)
+{
+    Plan pl;
+    int rc = make_plan(b, params, films, pl);
+    if (rc != LMGPU_OK) return rc;
+    int cur = 0;
+    LMGPU_CUDA_TRY(cudaGetDevice(&cur));
+    if (cur != b->device) return fail(LMGPU_ERR_INVALID, "batch used on another device than it was created on");
+    const int64_t P = std::min<int64_t>(b->cfg.wave_paths, pl.total);
+    if ((rc = ensure_batch_workspace(b, std::max<int64_t>(P, b->ws_capacity))) != LMGPU_OK) return rc;
+    if ((rc = upload_table(b, params, films, s)) != LMGPU_OK) return rc;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (stats) {
+        LMGPU_CUDA_TRY(cudaEventCreate(&e0));
+        LMGPU_CUDA_TRY(cudaEventCreate(&e1));
+        LMGPU_CUDA_TRY(cudaEventRecord(e0, s));
+    }
+    int64_t waves = 0;
+    rc = pl.fp64 ? dispatch_tech<double>(b, pl, P, s, waves) : dispatch_tech<float>(b, pl, P, s, waves);
+    if (stats) {
+        if (rc == LMGPU_OK) {
+            cudaError_t e = cudaEventRecord(e1, s);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_stats, b->d_stats, NSTATS * sizeof(unsigned long long),
+                                                      cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) rc = cuda_fail(e, "batch completion");
+        }
+        float ms = 0.0f;
+        if (rc == LMGPU_OK) cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        std::memset(stats, 0, sizeof(*stats));
+        if (rc == LMGPU_OK) {
+            stats->shadow_rays = (int64_t)b->h_stats[1];
+            stats->rays_traced = (int64_t)(b->h_stats[0] + b->h_stats[1]);
+            stats->paths = pl.total;
+            stats->waves = waves;
+            stats->max_bounces_run = (int32_t)b->h_stats[2];
+            stats->device_ms = ms;
+        }
+    }
+    if (rc == LMGPU_OK && stats) rc = consume_batch_status(b, s);
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lmgpu_batch_create(LmgpuScene* const* scenes, int32_t num_scenes, LmgpuBatch** out)
+{
+    if (!out) return fail(LMGPU_ERR_INVALID, "null output");
+    *out = nullptr;
+    if (!scenes || num_scenes <= 0) return fail(LMGPU_ERR_INVALID, "a batch needs at least one scene");
+    int dev = 0;
+    LMGPU_CUDA_TRY(cudaGetDevice(&dev));
+    for (int i = 0; i < num_scenes; i++) {
+        if (!scenes[i]) return fail(LMGPU_ERR_INVALID, "null scene");
+        if (scenes[i]->dev.layout == LMGPU_LAYOUT_NAIVE) return fail(LMGPU_ERR_INVALID, "batch scenes need a BVH layout");
+        if (scenes[i]->device != dev) return fail(LMGPU_ERR_INVALID, "batch scenes must live on the current device");
+    }
+    LmgpuBatch* b = new (std::nothrow) LmgpuBatch;
+    if (!b) return fail(LMGPU_ERR_OOM, "host allocation failed");
+    b->device = dev;
+    b->scenes.assign(scenes, scenes + num_scenes);
+    cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t n = (size_t)num_scenes;
+    cudaError_t e = cudaSuccess;
+    auto dm = [&](void** p, size_t bytes) { if (e == cudaSuccess) e = cudaMalloc(p, bytes); };
+    auto hm = [&](void** p, size_t bytes) { if (e == cudaSuccess) e = cudaMallocHost(p, bytes); };
+    dm(reinterpret_cast<void**>(&b->d_table), n * sizeof(BatchEntry));
+    dm(reinterpret_cast<void**>(&b->d_begins), (n + 1) * sizeof(int64_t));
+    dm(reinterpret_cast<void**>(&b->d_wave), sizeof(WaveCtl));
+    dm(reinterpret_cast<void**>(&b->d_stats), NSTATS * sizeof(unsigned long long));
+    dm(reinterpret_cast<void**>(&b->d_work), WORK_SLOTS * sizeof(unsigned long long));
+    dm(reinterpret_cast<void**>(&b->d_status), sizeof(int32_t));
+    hm(reinterpret_cast<void**>(&b->h_table), n * sizeof(BatchEntry));
+    hm(reinterpret_cast<void**>(&b->h_begins), (n + 1) * sizeof(int64_t));
+    hm(reinterpret_cast<void**>(&b->h_stats), NSTATS * sizeof(unsigned long long));
+    hm(reinterpret_cast<void**>(&b->h_counts), 16);
+    if (e == cudaSuccess) e = cudaMemset(b->d_status, 0, sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->staged, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        lmgpu_batch_destroy(b);
+        return e == cudaErrorMemoryAllocation ? fail(LMGPU_ERR_OOM, "batch allocation failed") : cuda_fail(e, "batch creation");
+    }
+    *out = b;
+    return LMGPU_OK;
+}
+
+int lmgpu_batch_destroy(LmgpuBatch* b)
+{
+    if (!b) return LMGPU_OK;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+    if (b->staged) cudaEventDestroy(b->staged);
+    cudaFree(b->ws_mem);
+    cudaFree(b->d_table);
+    cudaFree(b->d_begins);
+    cudaFree(b->d_wave);
+    cudaFree(b->d_stats);
+    cudaFree(b->d_work);
+    cudaFree(b->d_status);
+    cudaFreeHost(b->h_table);
+    cudaFreeHost(b->h_begins);
+    cudaFreeHost(b->h_stats);
+    cudaFreeHost(b->h_counts);
+    delete b;
+    return LMGPU_OK;
+}
+
+int lmgpu_batch_get_config(const LmgpuBatch* b, LmgpuBatchConfig* c)
+{
+    if (!b || !c) return fail(LMGPU_ERR_INVALID, "null argument");
+    *c = b->cfg;
+    return LMGPU_OK;
+}
+
+int lmgpu_batch_set_config(LmgpuBatch* b, const LmgpuBatchConfig* c)
+{
+    if (!b || !c) return fail(LMGPU_ERR_INVALID, "null argument");
+    const int rc = check_config(*c);
+    if (rc != LMGPU_OK) return rc;
+    b->cfg = *c;
+    b->cfg.use_graph = c->use_graph ? 1 : 0;
+    return LMGPU_OK;
+}
+
+int lmgpu_batch_render_device(LmgpuBatch* b, const LmgpuRenderParams* params, void* const* films, void* stream,
+                              LmgpuRenderStats* stats)
+{
+    if (!b || !params || !films) return fail(LMGPU_ERR_INVALID, "null argument");
+    return batch_render(b, params, films, static_cast<cudaStream_t>(stream), stats);
+}
+
+int lmgpu_batch_autotune(LmgpuBatch* b, const LmgpuRenderParams* params, double fraction, void* stream,
+                         LmgpuBatchConfig* chosen, double* best_ms)
+{
+    if (!b || !params) return fail(LMGPU_ERR_INVALID, "null argument");
+    if (!(fraction > 0.0 && fraction <= 1.0)) return fail(LMGPU_ERR_INVALID, "sample_fraction must be in (0, 1]");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t n = b->scenes.size();
+    // Scaled budgets, one scratch film shared by all scenes (its contents are discarded).
+    std::vector<LmgpuRenderParams> p(params, params + n);
+    int64_t px = 0, total = 0;
+    for (size_t i = 0; i < n; i++) {
+        p[i].num_samples = std::max<int64_t>(1, (int64_t)std::llround((double)params[i].num_samples * fraction));
+        total += p[i].num_samples;
+        px = std::max<int64_t>(px, (int64_t)b->scenes[i]->dev.cam.width * b->scenes[i]->dev.cam.height);
+    }
+    Plan pl;
+    int rc = make_plan(b, p.data(), nullptr, pl);
+    if (rc != LMGPU_OK) return rc;
+    void* film = nullptr;
+    const size_t esize = pl.fp64 ? sizeof(double) : sizeof(float);
+    LMGPU_CUDA_TRY(cudaMalloc(&film, std::max<int64_t>(px, 1) * 3 * esize));
+    std::vector<void*> films(n, film);
+
+    const LmgpuBatchConfig start = b->cfg;
+    auto trial = [&](const LmgpuBatchConfig& c, double& ms) -> int {
+        int r = check_config(c);
+        if (r != LMGPU_OK) return r;
+        b->cfg = c;
+        LmgpuRenderStats st;
+        if ((r = batch_render(b, p.data(), films.data(), s, &st)) != LMGPU_OK) return r;   // warm-up (capture)
+        double best = 1e30;
+        for (int k = 0; k < 2; k++) {
+            if ((r = batch_render(b, p.data(), films.data(), s, &st)) != LMGPU_OK) return r;
+            best = std::min(best, st.device_ms);
+        }
+        ms = best;
+        return LMGPU_OK;
+    };
+    LmgpuBatchConfig best = start;
+    best.use_graph = 1;
+    double best_t = 1e30;
+    rc = trial(best, best_t);
+    // Coordinate descent: layout, then wave size, then shading grid.
+    const int layouts[] = { LMGPU_LAYOUT_BVH2, LMGPU_LAYOUT_BVH4 };
+    const int waves[] = { 1 << 19, 1 << 20, 1 << 21, 1 << 22 };
+    const int grids[] = { 4, 8, 16 };
+    for (int l : layouts) {
+        if (rc != LMGPU_OK || l == best.layout) continue;
+        LmgpuBatchConfig c = best;
+        c.layout = l;
+        double t;
+        if ((rc = trial(c, t)) == LMGPU_OK && t < best_t) { best = c; best_t = t; }
+    }
+    int64_t largest = 0;
+    for (int w : waves) {
+        // Waves beyond the sample count behave like a wave of the sample count.
+        if (rc != LMGPU_OK || w == best.wave_paths || (w > total && largest >= total)) continue;
+        largest = std::max<int64_t>(largest, w);
+        LmgpuBatchConfig c = best;
+        c.wave_paths = w;
+        double t;
+        if ((rc = trial(c, t)) == LMGPU_OK && t < best_t) { best = c; best_t = t; }
+    }
+    for (int g : grids) {
+        if (rc != LMGPU_OK || g == best.shade_blocks_per_sm) continue;
+        LmgpuBatchConfig c = best;
+        c.shade_blocks_per_sm = g;
+        double t;
+        if ((rc = trial(c, t)) == LMGPU_OK && t < best_t) { best = c; best_t = t; }
+    }
+    cudaFree(film);
+    b->cfg = rc == LMGPU_OK ? best : start;
+    if (rc != LMGPU_OK) return rc;
+    if (chosen) *chosen = best;
+    if (best_ms) *best_ms = best_t;
+    return LMGPU_OK;
+}
+
+}  // extern "C"

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <mutex>
+#include <type_traits>
 #include <unordered_map>
 #include "internal.h"
 #include "trace.cuh"
@@ -12,8 +13,22 @@
 
 namespace lmgpu {
 
+// I/O policies whose rays each belong to their own scene (a multi-scene
+// batch) declare PER_RAY_SCENE = true and supply ray_scene(j).
+template <class IO, class = void>
+struct per_ray_scene : std::false_type {};
+template <class IO>
+struct per_ray_scene<IO, std::void_t<decltype(IO::PER_RAY_SCENE)>> : std::bool_constant<IO::PER_RAY_SCENE> {};
+
+// Node and triangle arrays of the scene a lane is tracing.
+struct LaneScene {
+    const Bvh2Node* bvh2;
+    const Bvh4Node* bvh4;
+    const TriRecord* tris;
+};
+
 template <int LAYOUT>
-__device__ __forceinline__ bool descend(const DeviceScene& s, TravState& ts, int2* stack, int cap, const TraversalRay& r)
+__device__ __forceinline__ bool descend(const LaneScene& s, TravState& ts, int2* stack, int cap, const TraversalRay& r)
 {
     if (LAYOUT == LMGPU_LAYOUT_BVH2) return bvh2_descend(s.bvh2, ts, stack, cap, r, nullptr);
     return bvh4_descend(s.bvh4, ts, stack, cap, r, nullptr);
@@ -26,6 +41,8 @@ __device__ __forceinline__ bool descend(const DeviceScene& s, TravState& ts, int
 // depth-first traversal as trace_bvh2 / trace_bvh4; only the scheduling
 // differs. Lanes alternate "descend to a leaf" and "test the leaf, pop"
 // (while-while) and refill when at least a quarter of the warp is idle.
+// For a multi-scene I/O policy each lane switches to its new ray's scene at
+// refill (node and triangle arrays, root); an empty scene is a miss.
 template <int LAYOUT, int STACK, bool ANY_HIT, class IO>
 __global__ void __launch_bounds__(128) k_trace_persistent(const DeviceScene s, const IO io, int32_t* status,
                                                           unsigned long long* next_ray)
@@ -35,6 +52,7 @@ __global__ void __launch_bounds__(128) k_trace_persistent(const DeviceScene s, c
     const int64_t n = io.count();
     const unsigned lane = threadIdx.x & 31u;
     const int32_t root = LAYOUT == LMGPU_LAYOUT_BVH2 ? s.root_ref : s.root_ref4;
+    LaneScene ls{ s.bvh2, s.bvh4, s.tris };
     TraversalRay r;
     Hit h;
     h.tri = -1;
@@ -57,7 +75,16 @@ __global__ void __launch_bounds__(128) k_trace_persistent(const DeviceScene s, c
                 if (idx < n) {
                     setup_ray(r, io.load(idx));
                     h.tri = -1;
-                    trav_begin(ts, root, s.root_box, r, nullptr);
+                    if constexpr (per_ray_scene<IO>::value) {
+                        const DeviceScene& rs = io.ray_scene(idx);
+                        ls.bvh2 = rs.bvh2;
+                        ls.bvh4 = rs.bvh4;
+                        ls.tris = rs.tris;
+                        if (rs.num_tris > 0)
+                            trav_begin(ts, LAYOUT == LMGPU_LAYOUT_BVH2 ? rs.root_ref : rs.root_ref4, rs.root_box, r, nullptr);
+                    } else {
+                        trav_begin(ts, root, s.root_box, r, nullptr);
+                    }
                     if (ts.ref == REF_DONE) io.store(idx, h, r);
                 }
             }
@@ -65,12 +92,12 @@ __global__ void __launch_bounds__(128) k_trace_persistent(const DeviceScene s, c
             break;
         }
         if (ts.ref != REF_DONE) {
-            if (!descend<LAYOUT>(s, ts, stack, STACK, r)) {
+            if (!descend<LAYOUT>(ls, ts, stack, STACK, r)) {
                 atomicOr(status, STATUS_STACK_OVERFLOW);
                 h.tri = -1;
                 ts.ref = REF_DONE;
             } else if (ts.ref != REF_DONE) {
-                if (trace_leaf<ANY_HIT>(s.tris, ~ts.ref, r, h, nullptr) && ANY_HIT) ts.ref = REF_DONE;
+                if (trace_leaf<ANY_HIT>(ls.tris, ~ts.ref, r, h, nullptr) && ANY_HIT) ts.ref = REF_DONE;
                 else pop_next(ts, stack, r, nullptr);
             }
             if (ts.ref == REF_DONE) io.store(idx, h, r);

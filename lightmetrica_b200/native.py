@@ -93,6 +93,11 @@ class RenderStats(ctypes.Structure):
 
 
 # Every symbol include/lmgpu.h declares, with (restype, argtypes).
+class BatchConfig(ctypes.Structure):
+    _fields_ = [("layout", c_int32), ("wave_paths", c_int32), ("shade_blocks_per_sm", c_int32),
+                ("use_graph", c_int32)]
+
+
 SIGNATURES = {
     "lmgpu_abi_version": (c_int32, []),
     "lmgpu_last_error": (ctypes.c_char_p, []),
@@ -112,6 +117,13 @@ SIGNATURES = {
     "lmgpu_adjoint_backward": (c_int32, [c_void_p, P(RenderParams), P(DiffParams), c_void_p, c_void_p, c_void_p,
                                          c_void_p, P(RenderStats)]),
     "lmgpu_intersect_counted": (c_int32, [c_void_p, P(RaysSoA), c_int64, P(HitsSoA), c_void_p, c_void_p]),
+    "lmgpu_batch_create": (c_int32, [P(c_void_p), c_int32, P(c_void_p)]),
+    "lmgpu_batch_destroy": (c_int32, [c_void_p]),
+    "lmgpu_batch_get_config": (c_int32, [c_void_p, P(BatchConfig)]),
+    "lmgpu_batch_set_config": (c_int32, [c_void_p, P(BatchConfig)]),
+    "lmgpu_batch_render_device": (c_int32, [c_void_p, P(RenderParams), P(c_void_p), c_void_p, P(RenderStats)]),
+    "lmgpu_batch_autotune": (c_int32, [c_void_p, P(RenderParams), c_double, c_void_p, P(BatchConfig),
+                                       P(c_double)]),
 }
 
 _lib = None

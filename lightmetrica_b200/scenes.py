@@ -230,3 +230,55 @@ def terrain_spheres(width: int = 1920, height: int = 1080, grid: int = 1024, sph
 
 def num_triangles(prims: Primitives) -> int:
     return int(sum(p.mesh.faces.shape[0] for p in prims.primitives if p.mesh is not None))
+
+
+# ----------------------------------------------------------- batch set ----
+
+BATCH_RESOLUTIONS = (128, 256, 512, 1024)
+
+
+def batch_scene(index: int, seed: int = 5) -> dict:
+    """Scene `index` of the seeded multi-scene set: a random-triangle soup or
+    a fBm heightfield with a log-uniform triangle count in [1k, 200k], a
+    square film from {128, 256, 512, 1024}, 4-64 spp, max depth 8-16, half
+    its triangles Lambertian and half perfect mirror, a 2-triangle area light
+    and a constant environment of 0.3. Returns {"prims", "spp",
+    "max_path_vertices", "kind", "triangles"}."""
+    rng = np.random.default_rng([seed, index])
+    tris = int(round(np.exp(rng.uniform(np.log(1e3), np.log(2e5)))))
+    res = int(rng.choice(BATCH_RESOLUTIONS))
+    spp = int(rng.choice((4, 8, 16, 32, 64)))
+    depth = int(rng.integers(8, 17))
+    kind = "soup" if index % 2 == 0 else "heightfield"
+    albedo = tuple(rng.uniform(0.2, 0.8, 3))
+    prims = Primitives()
+    if kind == "soup":
+        # Triangle size grows as the count falls, so that coverage stays comparable.
+        sigma = 0.01 * np.sqrt(float(1 << 20) / tris)
+        c = rng.uniform(-1.0, 1.0, size=(tris, 3))
+        e1 = rng.normal(0.0, sigma, size=(tris, 3))
+        e2 = rng.normal(0.0, sigma, size=(tris, 3))
+        v0 = c - (e1 + e2) / 3.0
+        P = np.stack([v0, v0 + e1, v0 + e2], axis=1).astype(np.float32)
+        half = tris // 2
+        for part, bsdf in ((P[:half], DiffuseBSDF(albedo)), (P[half:], PerfectMirrorBSDF((0.9, 0.9, 0.9)))):
+            k = part.shape[0]
+            if k == 0:
+                continue
+            prims.add(Primitive(mesh=TriangleMesh(part.reshape(-1, 3), np.arange(3 * k, dtype=np.uint32).reshape(-1, 3)),
+                                bsdf=bsdf))
+        light_y, light_half, eye, center = 1.6, 0.5, (0.0, 0.6, 3.4), (0.0, 0.0, 0.0)
+    else:
+        n = max(2, int(round(np.sqrt(tris / 2.0))) + 1)
+        hf = heightfield(n, extent=2.0, amplitude=0.25, seed=int(rng.integers(1 << 30)))
+        F = hf.faces
+        half = F.shape[0] // 2
+        prims.add(Primitive(mesh=TriangleMesh(hf.positions, F[:half], hf.normals), bsdf=DiffuseBSDF(albedo)))
+        prims.add(Primitive(mesh=TriangleMesh(hf.positions, F[half:], hf.normals), bsdf=PerfectMirrorBSDF((0.9, 0.9, 0.9))))
+        light_y, light_half, eye, center = 1.5, 0.6, (0.0, 1.6, 3.2), (0.0, 0.0, 0.0)
+    lp, ln, lf = _quad((-light_half, light_y, -light_half), (light_half, light_y, -light_half),
+                       (light_half, light_y, light_half), (-light_half, light_y, light_half), (0, -1, 0))
+    prims.add(Primitive(mesh=TriangleMesh(lp, lf, ln), bsdf=DiffuseBSDF((0.0, 0.0, 0.0)), light=AreaLight((12.0, 12.0, 12.0))))
+    prims.environment_light = ConstantEnvironmentLight((0.3, 0.3, 0.3))
+    prims.camera = PerspectiveCamera(fovy=45.0, eye=eye, center=center, up=(0, 1, 0), film=HDRBitmapFilm(res, res))
+    return {"prims": prims, "spp": spp, "max_path_vertices": depth + 1, "kind": kind, "triangles": num_triangles(prims)}

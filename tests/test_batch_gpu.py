@@ -1,0 +1,183 @@
+"""Multi-scene batch (lmgpu_batch_*): every scene of a batch must render the
+same paths as the one-scene renderer with the same parameters, whatever the
+batch configuration (BVH layout, wave size, shading grid, CUDA graph or
+direct launches). With FP64 films the two differ only in the order of the
+film additions, so they agree to ~1e-12 relative.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from lightmetrica_b200 import HDRBitmapFilm, create_renderer, create_scene, native, scenes
+from lightmetrica_b200.batch import SceneBatch
+
+pytestmark = pytest.mark.gpu
+
+
+def build(prims, layout="bvh"):
+    s = create_scene(layout)
+    s.load(prims)
+    s.configure({})
+    s.build()
+    return s
+
+
+def renderer(technique, rr_depth, max_pv, seed):
+    r = create_renderer(technique)
+    r.configure({"rr_depth": rr_depth, "max_path_vertices": max_pv, "sampler": {"rng_seed": seed}})
+    return r
+
+
+def small_set(technique="pt.mis"):
+    """Scenes of different sizes, depths, seeds and sample counts."""
+    items = []
+    items.append((scenes.cornell_box(64, 64), renderer(technique, 3, 9, 1), 64 * 64 * 16))
+    items.append((scenes.cornell_box(48, 40, variant="mixed"), renderer(technique, 2, 6, 7), 48 * 40 * 24))
+    for i in range(4):
+        d = scenes.batch_scene(i, seed=11)
+        d["prims"].camera.film = HDRBitmapFilm(40 + 8 * i, 32 + 8 * i)
+        W, H = d["prims"].camera.film.width, d["prims"].camera.film.height
+        items.append((d["prims"], renderer(technique, 4, d["max_path_vertices"], 3 + i), W * H * (4 + 2 * i)))
+    return items
+
+
+def plain_films(built, items):
+    import torch
+    out = []
+    for sc, (prims, r, n) in zip(built, items):
+        W, H = prims.camera.film.width, prims.camera.film.height
+        f = torch.zeros(W * H * 3, dtype=torch.float64, device="cuda")
+        p = r.params(n, film_fp64=True)
+        st = native.RenderStats()
+        native.check(native.lib().lmgpu_render_device(sc.handle, ctypes.byref(p), ctypes.c_void_p(f.data_ptr()),
+                                                      ctypes.c_void_p(torch.cuda.current_stream().cuda_stream),
+                                                      ctypes.byref(st)))
+        out.append(f)
+    torch.cuda.synchronize()
+    return [f.cpu().numpy() for f in out]
+
+
+def batch_films(batch, items):
+    import torch
+    films = [torch.zeros(p.camera.film.width * p.camera.film.height * 3, dtype=torch.float64, device="cuda")
+             for p, _, _ in items]
+    batch.render_device([r for _, r, _ in items], [n for _, _, n in items], films)
+    torch.cuda.synchronize()
+    return [f.cpu().numpy() for f in films]
+
+
+def assert_same(got, want):
+    for g, w in zip(got, want):
+        assert w.max() > 0
+        np.testing.assert_allclose(g, w, rtol=1e-9, atol=1e-12)
+
+
+@pytest.mark.parametrize("technique", ["pt.mis", "pt.direct", "pt"])
+def test_batch_matches_one_scene_renders(cuda, technique):
+    items = small_set(technique)
+    built = [build(p) for p, _, _ in items]
+    want = plain_films(built, items)
+    batch = SceneBatch(built)
+    assert_same(batch_films(batch, items), want)
+    st = batch.last_stats
+    assert st["paths"] == sum(n for _, _, n in items)
+    assert st["rays_traced"] > st["paths"] // 2 and st["max_bounces_run"] >= 5
+    batch.close()
+
+
+@pytest.mark.parametrize("config", [
+    dict(layout="qbvh"),
+    dict(wave_paths=4096),                       # many waves, every wave spans scenes
+    dict(wave_paths=1 << 20, shade_blocks_per_sm=2),
+    dict(use_graph=False),
+    dict(layout="qbvh", wave_paths=10000, use_graph=False),
+])
+def test_batch_configurations_agree(cuda, config):
+    items = small_set()
+    built = [build(p) for p, _, _ in items]
+    want = plain_films(built, items)
+    batch = SceneBatch(built)
+    batch.configure(**config)
+    assert_same(batch_films(batch, items), want)
+    assert_same(batch_films(batch, items), want)     # graph replay with a fresh table
+    batch.close()
+
+
+def test_batch_unbounded_depth_tail(cuda):
+    """max_path_vertices = -1 (Russian roulette only): the graph covers the
+    first bounces and direct launches finish the deep tail."""
+    items = [(scenes.cornell_box(32, 32, variant="mixed"), renderer("pt.mis", 1, -1, 5), 32 * 32 * 32),
+             (scenes.cornell_box(24, 24), renderer("pt.mis", 1, -1, 6), 24 * 24 * 16)]
+    built = [build(p) for p, _, _ in items]
+    want = plain_films(built, items)
+    batch = SceneBatch(built)
+    batch.configure(wave_paths=8192)
+    assert_same(batch_films(batch, items), want)
+    batch.close()
+
+
+def test_batch_repeated_scene_and_sample_offsets(cuda):
+    """One scene twice with disjoint sample ranges equals one render of both ranges."""
+    import torch
+    prims = scenes.cornell_box(32, 32)
+    sc = build(prims)
+    r = renderer("pt.mis", 3, 9, 2)
+    n = 32 * 32 * 8
+    batch = SceneBatch([sc, sc])
+    p = (native.RenderParams * 2)(r.params(n, film_fp64=True), r.params(n, sample_offset=n, film_fp64=True))
+    f = torch.zeros(32 * 32 * 3, dtype=torch.float64, device="cuda")
+    ptrs = (ctypes.c_void_p * 2)(f.data_ptr(), f.data_ptr())
+    native.check(native.lib().lmgpu_batch_render_device(batch.handle, p, ptrs, None, None))
+    torch.cuda.synchronize()
+    want = plain_films([sc], [(prims, r, 2 * n)])[0]
+    np.testing.assert_allclose(f.cpu().numpy(), want, rtol=1e-9, atol=1e-12)
+    batch.close()
+
+
+def test_batch_autotune_keeps_results(cuda):
+    items = small_set()
+    built = [build(p) for p, _, _ in items]
+    want = plain_films(built, items)
+    batch = SceneBatch(built)
+    cfg = batch.autotune([r for _, r, _ in items], [n for _, _, n in items], sample_fraction=0.25)
+    assert cfg["layout"] in ("bvh", "qbvh") and cfg["trial_ms"] > 0
+    assert cfg["wave_paths"] in (1 << 19, 1 << 20, 1 << 21, 1 << 22)
+    assert_same(batch_films(batch, items), want)
+    batch.close()
+
+
+def test_batch_rescaled_render_matches_scheduler(cuda):
+    from lightmetrica_b200 import create_scheduler
+    items = small_set()[:3]
+    built = [build(p) for p, _, _ in items]
+    batch = SceneBatch(built)
+    films = batch.render([r for _, r, _ in items], [n for _, _, n in items])
+    for sc, (prims, r, n), f in zip(built, items, films):
+        s = create_scheduler("mt")
+        s.configure({"num_samples": n})
+        np.testing.assert_allclose(f, s.render(r, sc), rtol=2e-4, atol=1e-5)
+    batch.close()
+
+
+def test_batch_errors(cuda):
+    import torch
+    L = native.lib()
+    a, b = build(scenes.cornell_box(16, 16)), build(scenes.cornell_box(16, 16))
+    naive = build(scenes.cornell_box(16, 16), layout="naive")
+    h = ctypes.c_void_p()
+    assert L.lmgpu_batch_create((ctypes.c_void_p * 1)(naive.handle.value), 1, ctypes.byref(h)) == native.ERR_INVALID
+    assert L.lmgpu_batch_create(None, 0, ctypes.byref(h)) == native.ERR_INVALID
+    batch = SceneBatch([a, b])
+    f = torch.zeros(16 * 16 * 3, device="cuda")
+    ptrs = (ctypes.c_void_p * 2)(f.data_ptr(), f.data_ptr())
+    p = (native.RenderParams * 2)(renderer("pt.mis", 3, 9, 1).params(256), renderer("pt", 3, 9, 1).params(256))
+    assert L.lmgpu_batch_render_device(batch.handle, p, ptrs, None, None) == native.ERR_INVALID
+    assert b"one technique" in L.lmgpu_last_error()
+    p[1] = renderer("pt.mis", 3, 9, 1).params(0)
+    assert L.lmgpu_batch_render_device(batch.handle, p, ptrs, None, None) == native.ERR_INVALID
+    with pytest.raises(native.LmgpuError):
+        batch.configure(wave_paths=16)
+    with pytest.raises(ValueError):
+        batch.configure(layout="naive")
+    batch.close()
