@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
     ap.add_argument("--rays-log2", type=int, default=24, help="ray batch 2^k (profiling runs use less)")
+    ap.add_argument("--render-spp", type=int, default=64, help="spp of the 1080p section (profiling runs use less)")
+    ap.add_argument("--render-frames", type=int, default=3, help="timed frames of the 1080p section")
     ap.add_argument("--sections", default="render,adjoint,batch",
                     help="extra single-GPU sections in the same line: render (1080p path tracer), "
                          "adjoint (forward/backward cost), batch (64-scene batch vs plain); '' for none")
@@ -348,7 +350,7 @@ def run_ours(args):
 
 # ------------------------------------------------------------- sections ----
 
-TERRAIN_W, TERRAIN_H, TERRAIN_SPP = 1920, 1080, 64
+TERRAIN_W, TERRAIN_H = 1920, 1080
 TERRAIN_RR, TERRAIN_MAX_PV = 5, 17       # Russian roulette after depth 4, max depth 16
 
 
@@ -379,7 +381,7 @@ def render_section(args, dev, cpu_baseline):
     import torch
     from lightmetrica_b200 import create_renderer, create_scene, create_scheduler, native, scenes
     L = native.lib()
-    W, H, S = TERRAIN_W, TERRAIN_H, TERRAIN_SPP
+    W, H, S = TERRAIN_W, TERRAIN_H, args.render_spp
     t0 = time.perf_counter()
     prims = scenes.terrain_spheres(W, H)
     gen_s = time.perf_counter() - t0
@@ -394,7 +396,7 @@ def render_section(args, dev, cpu_baseline):
     film = torch.zeros(W * H * 3, dtype=torch.float32, device=dev)
     n = W * H * S
     _timed_device_renders(L, scene, r, n, film, stream, 1, native)          # warm-up
-    runs = _timed_device_renders(L, scene, r, n, film, stream, 3, native)
+    runs = _timed_device_renders(L, scene, r, n, film, stream, max(1, args.render_frames), native)
     scene.status(stream.cuda_stream)
     ms = sum(x[0] for x in runs) / len(runs)
     rays = sum(x[1] for x in runs) / len(runs)

@@ -3,7 +3,10 @@
 CUDA sources are compiled for sm_100a only
 (-gencode arch=compute_100a,code=sm_100a); the host BVH builder is compiled by
 the system g++ with -ffp-contract=off so that its float arithmetic rounds
-each operation separately, like the reference's float SSE build.
+each operation separately, like the reference's float SSE build. Device code
+is compiled with --fmad=false for the same reason: no multiply-add is fused
+behind the source's back, so a kernel instantiated in two contexts (one
+scene, a scene batch) computes every path bit for bit the same.
 """
 from __future__ import annotations
 
@@ -21,7 +24,7 @@ BUILD_DIR = os.path.join(HERE, "_build")
 CU_SOURCES = ["api.cu", "pathtrace.cu", "adjoint.cu", "noalloc.cu", "batch.cu"]
 CPP_SOURCES = ["builder.cpp"]
 HEADERS = ["layout.h", "builder.h", "internal.h", "scene.cuh", "trace.cuh", "trace4.cuh",
-           "shading.cuh", "rng.cuh", "pathtrace.cuh", "trace_kernels.cuh"]
+           "shading.cuh", "rng.cuh", "pathtrace.cuh", "trace_kernels.cuh", "pt_kernels.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -46,7 +49,9 @@ def _stale(obj, deps):
 def build(verbose: bool = False, ptxas_verbose: bool = False) -> str:
     os.makedirs(OUT_DIR, exist_ok=True)
     os.makedirs(BUILD_DIR, exist_ok=True)
-    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(os.path.dirname(HERE), "include", "lmgpu.h")]
+    # This file's flags are a dependency of every object too.
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(os.path.dirname(HERE), "include", "lmgpu.h"),
+                                                       os.path.abspath(__file__)]
     objs = []
     procs = []
     for src in CU_SOURCES:
@@ -57,7 +62,7 @@ def build(verbose: bool = False, ptxas_verbose: bool = False) -> str:
         objs.append(o)
         if _stale(o, [s] + hdrs):
             cmd = [_nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
-                   "-Xcompiler", "-ffp-contract=off", "--expt-relaxed-constexpr",
+                   "-Xcompiler", "-ffp-contract=off", "--fmad=false", "--expt-relaxed-constexpr",
                    "-ccbin", _cxx(), "-c", s, "-o", o]
             if ptxas_verbose:
                 cmd.insert(1, "-Xptxas=-v")

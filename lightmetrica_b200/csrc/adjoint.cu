@@ -8,7 +8,13 @@
 // and, for each radiance contribution c splatted at pixel p, adds
 // dL/dI_p * c / R_t to the gradient of the albedo R of every diffuse vertex t
 // on the contribution's prefix (c is linear in each of them) and
-// dL/dI_p * c / Le to the emission of its light. Russian-roulette
+// dL/dI_p * c / Le to the emission of its light. A path's contributions come
+// in order of non-decreasing prefix length, so the replay keeps, per vertex,
+// the sum of the weights w = dL/dI_p * c whose prefix ends there and turns
+// them into suffix sums once the path is done: one set of atomics per
+// vertex instead of one per (contribution, vertex). Emission gradients are
+// summed per thread and per block before they reach global memory, since
+// every path adds to the same few lights. Russian-roulette
 // probabilities and MIS weights are held at their sampled values, which keeps
 // the estimator unbiased for the diffuse BSDFs (their sampling densities do
 // not depend on R). Per-vertex records live in a fixed local array
@@ -87,14 +93,35 @@ __device__ __forceinline__ V3 light_Le(const DeviceScene& s, const DiffConsts& c
 
 struct Replay {
     int32_t tri[MAX_REPLAY_VERTS];
+    V3 w[MAX_REPLAY_VERTS];   // adjoint: weights of the contributions whose prefix ends at this vertex
     int n;
 };
 
-// One contribution: forward splats it, the adjoint distributes dL/dI . c.
+// Emission gradient of one light summed by a thread; flushed into the
+// block's shared sums (lights below SHARED_LIGHTS) or to global memory.
+constexpr int SHARED_LIGHTS = 32;
+struct EmissionSum {
+    int light;
+    V3 g;
+};
+
+__device__ __forceinline__ void flush_emission(EmissionSum& e, float* s_de, float* d_emission)
+{
+    if (e.light < 0) return;
+    float* dst = e.light < SHARED_LIGHTS ? s_de + 3 * e.light : d_emission + 3 * e.light;
+    if (e.g.x != 0.0f) atomicAdd(dst, e.g.x);
+    if (e.g.y != 0.0f) atomicAdd(dst + 1, e.g.y);
+    if (e.g.z != 0.0f) atomicAdd(dst + 2, e.g.z);
+    e.light = -1;
+    e.g = v3(0, 0, 0);
+}
+
+// One contribution: forward splats it, the adjoint records dL/dI . c for the
+// albedos of its prefix (prefix length `depth`) and for its light.
 template <bool BACKWARD>
-__device__ __forceinline__ void contribute(const DiffConsts& c, const DeviceScene& s, const Replay& rp, int depth,
+__device__ __forceinline__ void contribute(const DiffConsts& c, const DeviceScene& s, Replay& rp, int depth,
                                            int light, int pixel, V3 contrib, float* image, const float* dL,
-                                           float* d_albedo, float* d_emission)
+                                           EmissionSum& es, float* s_de, float* d_emission)
 {
     if (pixel < 0 || is_zero(contrib)) return;
     if (!BACKWARD) {
@@ -105,19 +132,31 @@ __device__ __forceinline__ void contribute(const DiffConsts& c, const DeviceScen
     }
     const V3 w = v3(dL[3 * pixel] * contrib.x, dL[3 * pixel + 1] * contrib.y, dL[3 * pixel + 2] * contrib.z) * c.scale;
     if (is_zero(w)) return;
-    for (int i = 0; i < depth && i < rp.n; i++) {
+    if (depth > 0) rp.w[depth - 1] = rp.w[depth - 1] + w;
+    if (light >= 0 && light < s.num_area_lights) {
+        const V3 Le = light_Le(s, c, light);
+        const V3 g = v3(Le.x != 0.0f ? w.x / Le.x : 0.0f, Le.y != 0.0f ? w.y / Le.y : 0.0f,
+                        Le.z != 0.0f ? w.z / Le.z : 0.0f);
+        if (es.light != light) flush_emission(es, s_de, d_emission);
+        es.light = light;
+        es.g = es.g + g;
+    }
+}
+
+// End of a replayed path: vertex i's albedo gradient is the sum of the
+// weights of every contribution whose prefix contains it (suffix sums).
+__device__ __forceinline__ void flush_albedo(const DiffConsts& c, const DeviceScene& s, const Replay& rp, float* d_albedo)
+{
+    V3 S = v3(0, 0, 0);
+    for (int i = rp.n - 1; i >= 0; i--) {
+        S = S + rp.w[i];
+        if (is_zero(S)) continue;
         const int t = rp.tri[i];
         const Material m = diff_material(s, c, t);
         if (m.type != LMGPU_BSDF_DIFFUSE) continue;
-        if (m.R.x != 0.0f) atomicAdd(d_albedo + 3 * (int64_t)t, w.x / m.R.x);
-        if (m.R.y != 0.0f) atomicAdd(d_albedo + 3 * (int64_t)t + 1, w.y / m.R.y);
-        if (m.R.z != 0.0f) atomicAdd(d_albedo + 3 * (int64_t)t + 2, w.z / m.R.z);
-    }
-    if (light >= 0 && light < s.num_area_lights) {
-        const V3 Le = light_Le(s, c, light);
-        if (Le.x != 0.0f) atomicAdd(d_emission + 3 * light, w.x / Le.x);
-        if (Le.y != 0.0f) atomicAdd(d_emission + 3 * light + 1, w.y / Le.y);
-        if (Le.z != 0.0f) atomicAdd(d_emission + 3 * light + 2, w.z / Le.z);
+        if (m.R.x != 0.0f) atomicAdd(d_albedo + 3 * (int64_t)t, S.x / m.R.x);
+        if (m.R.y != 0.0f) atomicAdd(d_albedo + 3 * (int64_t)t + 1, S.y / m.R.y);
+        if (m.R.z != 0.0f) atomicAdd(d_albedo + 3 * (int64_t)t + 2, S.z / m.R.z);
     }
 }
 
@@ -137,6 +176,14 @@ __global__ void __launch_bounds__(128) k_diff(const DeviceScene s, const DiffCon
 {
     int2 stack[STACK];
     Replay rp;
+    __shared__ float s_de[3 * SHARED_LIGHTS];
+    EmissionSum es;
+    es.light = -1;
+    es.g = v3(0, 0, 0);
+    if (BACKWARD) {
+        for (int i = threadIdx.x; i < 3 * SHARED_LIGHTS; i += blockDim.x) s_de[i] = 0.0f;
+        __syncthreads();
+    }
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < c.num_samples; j += stride) {
         const uint64_t sample = (uint64_t)(c.sample_offset + j);
@@ -176,7 +223,7 @@ __global__ void __launch_bounds__(128) k_diff(const DeviceScene s, const DiffCon
                         float w = 1.0f;
                         if (TECH == LMGPU_RENDER_PT_MIS) { const float pdl = lp.pdf_area / G; w = pdl / (pdl + We); }
                         contribute<BACKWARD>(c, s, rp, 0, li, film_pixel(s.cam, lrx, lry), Le * (w * We * G / lp.pdf_area),
-                                             image, dL, d_albedo, d_emission);
+                                             image, dL, es, s_de, d_emission);
                     }
                 }
             }
@@ -217,19 +264,25 @@ __global__ void __launch_bounds__(128) k_diff(const DeviceScene s, const DiffCon
                 }
                 m = diff_material(s, c, tri);
                 surface = true;
-                if (rp.n < MAX_REPLAY_VERTS) rp.tri[rp.n++] = tri;
-                else { atomicOr(status, STATUS_QUEUE_OVERFLOW); break; }
+                if (rp.n < MAX_REPLAY_VERTS) {
+                    rp.tri[rp.n] = tri;
+                    if (BACKWARD) rp.w[rp.n] = v3(0, 0, 0);
+                    rp.n++;
+                } else {
+                    atomicOr(status, STATUS_QUEUE_OVERFLOW);
+                    break;
+                }
             }
             const int depth_here = rp.n - (surface ? 1 : 0);
             if (!is_zero(Le)) {
                 const V3 contrib = thr * Le;
                 if (TECH == LMGPU_RENDER_PT || prev_spec) {
-                    contribute<BACKWARD>(c, s, rp, depth_here, light, path_pixel, contrib, image, dL, d_albedo, d_emission);
+                    contribute<BACKWARD>(c, s, rp, depth_here, light, path_pixel, contrib, image, dL, es, s_de, d_emission);
                 } else if (TECH == LMGPU_RENDER_PT_MIS) {
                     const float G = geometry_term(prev_p, prev_n, prev_deg, g.p, g.sn, false);
                     const float pdl = G == 0.0f ? 0.0f : lpdf / (float(s.num_lights) * G);
                     contribute<BACKWARD>(c, s, rp, depth_here, light, path_pixel, contrib * (prev_pdf / (prev_pdf + pdl)),
-                                         image, dL, d_albedo, d_emission);
+                                         image, dL, es, s_de, d_emission);
                 }
             }
             if (!surface) break;
@@ -249,7 +302,7 @@ __global__ void __launch_bounds__(128) k_diff(const DeviceScene s, const DiffCon
                         float w = 1.0f;
                         if (TECH == LMGPU_RENDER_PT_MIS) { const float pdl = lp.pdf_area / G; w = pdl / (pdl + pb); }
                         contribute<BACKWARD>(c, s, rp, rp.n, li, path_pixel, thr * fs * Lel * (w * G / lp.pdf_area),
-                                             image, dL, d_albedo, d_emission);
+                                             image, dL, es, s_de, d_emission);
                     }
                 }
             }
@@ -273,6 +326,14 @@ __global__ void __launch_bounds__(128) k_diff(const DeviceScene s, const DiffCon
             prev_p = g.p; prev_n = g.sn; prev_deg = false; prev_spec = bs.specular; prev_pdf = bs.pdf;
             ro = g.p; rd = bs.wo; tmin = EPS_F;
         }
+        if (BACKWARD) flush_albedo(c, s, rp, d_albedo);
+    }
+    if (BACKWARD) {
+        flush_emission(es, s_de, d_emission);
+        __syncthreads();
+        const int n = 3 * min(s.num_area_lights, SHARED_LIGHTS);
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+            if (s_de[i] != 0.0f) atomicAdd(d_emission + i, s_de[i]);
     }
 }
 
