@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--rays-log2", type=int, default=24, help="ray batch 2^k (profiling runs use less)")
     ap.add_argument("--render-spp", type=int, default=64, help="spp of the 1080p section (profiling runs use less)")
     ap.add_argument("--render-frames", type=int, default=3, help="timed frames of the 1080p section")
+    ap.add_argument("--no-render-parity", action="store_true", help="skip the 1080p section's relMSE image")
     ap.add_argument("--sections", default="render,adjoint,batch",
                     help="extra single-GPU sections in the same line: render (1080p path tracer), "
                          "adjoint (forward/backward cost), batch (64-scene batch vs plain); '' for none")
@@ -411,17 +412,9 @@ def render_section(args, dev, cpu_baseline):
 
     # Parity at the scaled-down size against the FP64 reference image.
     gold = np.load(os.path.join(ROOT, "tests", "golden", "terrain_ref_mis_96x54.npz"))
-    small = scenes.terrain_spheres(96, 54)
-    sc = create_scene(args.layout)
-    sc.load(small)
-    sc.configure({})
-    sc.build()
-    sched = create_scheduler("mt")
-    sched.configure({"num_samples": 96 * 54 * 65536})
-    img = sched.render(r, sc)
-    sc.close()
-    ref = gold["film"].astype(np.float64)
-    rel = float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+    rel = None
+    if not args.no_render_parity:
+        rel = _terrain_parity(args, r, gold)
 
     out = {
         "workload": f"full path tracer: {scenes.num_triangles(prims):,}-triangle fBm heightfield + 64 level-5 "
@@ -443,6 +436,23 @@ def render_section(args, dev, cpu_baseline):
     if cpu_baseline:
         out["cpu_baseline"] = _render_cpu_baseline(prims, n)
     return out
+
+
+def _terrain_parity(args, r, gold):
+    """relMSE of the terrain scene at 96 x 54 (65,536 spp) against the
+    reference's FP64 image of the same scene and camera."""
+    from lightmetrica_b200 import create_scene, create_scheduler, scenes
+    small = scenes.terrain_spheres(96, 54)
+    sc = create_scene(args.layout)
+    sc.load(small)
+    sc.configure({})
+    sc.build()
+    sched = create_scheduler("mt")
+    sched.configure({"num_samples": 96 * 54 * 65536})
+    img = sched.render(r, sc)
+    sc.close()
+    ref = gold["film"].astype(np.float64)
+    return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
 
 
 def _render_cpu_baseline(prims, gpu_samples):
