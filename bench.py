@@ -137,13 +137,17 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def load_traffic(layout):
-    """Per-launch DRAM bytes of the traversal kernel from the committed ncu
-    summary (profiles/), or None."""
-    p = os.path.join(ROOT, "profiles", f"trace_closest_{layout}_intersect.json")
+def load_traffic(layout, num_rays):
+    """DRAM bytes (read + write) of one full-size traversal launch, from the
+    committed ncu summary of the kernel (profiles/): its line
+    `dram_bytes_per_ray: X` (measured on a smaller capture, scaled by the
+    rays of this launch), or None."""
+    p = os.path.join(ROOT, "profiles", f"trace_closest_{layout}_intersect.md")
     if os.path.exists(p):
         with open(p) as f:
-            return json.load(f).get("dram_bytes_per_launch_full")
+            for line in f:
+                if line.startswith("dram_bytes_per_ray:"):
+                    return int(float(line.split(":", 1)[1]) * num_rays)
     return None
 
 
@@ -310,7 +314,7 @@ def run_ours(args):
     peak, peak_kind = measured_peaks()
     avg_launch_ms = sum(launch_ms) / len(launch_ms)
     achieved = bytes_per_ray * n / (avg_launch_ms / 1e3) / 1e9
-    traffic = load_traffic(args.layout)
+    traffic = load_traffic(args.layout, n)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
