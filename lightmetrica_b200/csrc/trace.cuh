@@ -174,11 +174,19 @@ __device__ __forceinline__ void trav_begin(TravState& ts, int32_t root_ref, cons
 }
 
 // Binary children-in-parent nodes: descends until the state reaches a leaf
-// or finishes. Returns false on stack overflow.
+// or finishes. Returns false on stack overflow. With EXIT_BELOW > 0 and
+// `may_exit`, it also returns (state intact, at an internal node) once fewer
+// than EXIT_BELOW lanes of the warp are still descending, after at least one
+// step: the caller resumes it later, so the ray's walk is unchanged.
+template <int EXIT_BELOW = 0>
 __device__ __forceinline__ bool bvh2_descend(const Bvh2Node* __restrict__ nodes, TravState& ts, int2* stack,
-                                             int stack_cap, const TraversalRay& r, TraceStats* st)
+                                             int stack_cap, const TraversalRay& r, TraceStats* st,
+                                             bool may_exit = false)
 {
+    bool stepped = false;
     while (ts.ref >= 0 && ts.ref != REF_DONE) {
+        if (EXIT_BELOW > 0 && may_exit && stepped && __popc(__activemask()) < EXIT_BELOW) break;
+        stepped = true;
         const float4* np = reinterpret_cast<const float4*>(nodes + ts.ref);
         const float4 bx = __ldg(np), by = __ldg(np + 1), bz = __ldg(np + 2);
         const int4 meta = __ldg(reinterpret_cast<const int4*>(np + 3));

@@ -14,11 +14,16 @@
 namespace lmgpu {
 
 // 4-wide nodes: descends until the state reaches a leaf or finishes.
-// Returns false on stack overflow.
+// Returns false on stack overflow. EXIT_BELOW / may_exit as in bvh2_descend.
+template <int EXIT_BELOW = 0>
 __device__ __forceinline__ bool bvh4_descend(const Bvh4Node* __restrict__ nodes, TravState& ts, int2* stack,
-                                             int stack_cap, const TraversalRay& r, TraceStats* st)
+                                             int stack_cap, const TraversalRay& r, TraceStats* st,
+                                             bool may_exit = false)
 {
+    bool stepped = false;
     while (ts.ref >= 0 && ts.ref != REF_DONE) {
+        if (EXIT_BELOW > 0 && may_exit && stepped && __popc(__activemask()) < EXIT_BELOW) break;
+        stepped = true;
         const float4* np = reinterpret_cast<const float4*>(nodes + ts.ref);
         const float4 lox = __ldg(np + 0), hix = __ldg(np + 1);
         const float4 loy = __ldg(np + 2), hiy = __ldg(np + 3);

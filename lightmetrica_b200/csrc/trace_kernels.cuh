@@ -27,11 +27,25 @@ struct LaneScene {
     const TriRecord* tris;
 };
 
+// Scheduling constants of the persistent traversal kernel. They change only
+// when lanes take new rays and when a descent pauses, never a ray's walk.
+#ifndef LMGPU_TRACE_REFILL_MIN
+#define LMGPU_TRACE_REFILL_MIN 8      // idle lanes that trigger a refill
+#endif
+#ifndef LMGPU_TRACE_EXIT_BELOW
+#define LMGPU_TRACE_EXIT_BELOW 0      // pause a descent when fewer lanes descend (0: never)
+#endif
+#ifndef LMGPU_TRACE_MIN_BLOCKS
+#define LMGPU_TRACE_MIN_BLOCKS 1      // minimum resident blocks of 128 threads per SM
+#endif
+
 template <int LAYOUT>
-__device__ __forceinline__ bool descend(const LaneScene& s, TravState& ts, int2* stack, int cap, const TraversalRay& r)
+__device__ __forceinline__ bool descend(const LaneScene& s, TravState& ts, int2* stack, int cap, const TraversalRay& r,
+                                        bool may_exit)
 {
-    if (LAYOUT == LMGPU_LAYOUT_BVH2) return bvh2_descend(s.bvh2, ts, stack, cap, r, nullptr);
-    return bvh4_descend(s.bvh4, ts, stack, cap, r, nullptr);
+    if (LAYOUT == LMGPU_LAYOUT_BVH2)
+        return bvh2_descend<LMGPU_TRACE_EXIT_BELOW>(s.bvh2, ts, stack, cap, r, nullptr, may_exit);
+    return bvh4_descend<LMGPU_TRACE_EXIT_BELOW>(s.bvh4, ts, stack, cap, r, nullptr, may_exit);
 }
 
 // Persistent traversal with per-lane ray replacement: a warp keeps tracing
@@ -44,7 +58,7 @@ __device__ __forceinline__ bool descend(const LaneScene& s, TravState& ts, int2*
 // For a multi-scene I/O policy each lane switches to its new ray's scene at
 // refill (node and triangle arrays, root); an empty scene is a miss.
 template <int LAYOUT, int STACK, bool ANY_HIT, class IO>
-__global__ void __launch_bounds__(128) k_trace_persistent(const DeviceScene s, const IO io, int32_t* status,
+__global__ void __launch_bounds__(128, LMGPU_TRACE_MIN_BLOCKS) k_trace_persistent(const DeviceScene s, const IO io, int32_t* status,
                                                           unsigned long long* next_ray)
 {
     constexpr unsigned FULL = 0xffffffffu;
@@ -64,7 +78,7 @@ __global__ void __launch_bounds__(128) k_trace_persistent(const DeviceScene s, c
     for (;;) {
         const bool idle = ts.ref == REF_DONE;
         const unsigned need = __ballot_sync(FULL, idle);
-        if (!exhausted && (__popc(need) >= 8 || need == FULL)) {
+        if (!exhausted && (__popc(need) >= LMGPU_TRACE_REFILL_MIN || need == FULL)) {
             const int leader = __ffs(need) - 1;
             unsigned long long base = 0;
             if ((int)lane == leader) base = atomicAdd(next_ray, (unsigned long long)__popc(need));
@@ -92,11 +106,11 @@ __global__ void __launch_bounds__(128) k_trace_persistent(const DeviceScene s, c
             break;
         }
         if (ts.ref != REF_DONE) {
-            if (!descend<LAYOUT>(ls, ts, stack, STACK, r)) {
+            if (!descend<LAYOUT>(ls, ts, stack, STACK, r, !exhausted)) {
                 atomicOr(status, STATUS_STACK_OVERFLOW);
                 h.tri = -1;
                 ts.ref = REF_DONE;
-            } else if (ts.ref != REF_DONE) {
+            } else if (ts.ref < 0) {           // at a leaf (a paused descent resumes next round)
                 if (trace_leaf<ANY_HIT>(ls.tris, ~ts.ref, r, h, nullptr) && ANY_HIT) ts.ref = REF_DONE;
                 else pop_next(ts, stack, r, nullptr);
             }
