@@ -259,9 +259,14 @@ __global__ void __launch_bounds__(128) k_pt_init(const Ctx ctx, const PathState 
 
 // Closest-hit traversal of the queued rays (writes hit records). With a
 // scene table each ray is traced in its own path's scene.
+// Both path-tracer queues refill traversal lanes 24 at a time (measured on
+// the 1080p terrain: a few percent faster than 8).
+constexpr int PATH_QUEUE_REFILL_MIN = 24;
+
 template <bool TABLE>
 struct PathRayIO {
     static constexpr bool PER_RAY_SCENE = TABLE;
+    static constexpr int REFILL_MIN = PATH_QUEUE_REFILL_MIN;
     const int32_t* queue;
     const uint32_t* count_ptr;
     const float4* ray_o;
@@ -293,6 +298,7 @@ struct PathRayIO {
 template <class Ctx>
 struct ShadowIO {
     static constexpr bool PER_RAY_SCENE = Ctx::TABLE;
+    static constexpr int REFILL_MIN = PATH_QUEUE_REFILL_MIN;
     const uint32_t* count_ptr;
     const float4* sh_o;
     const float4* sh_d;
