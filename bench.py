@@ -142,7 +142,8 @@ def load_traffic(layout, num_rays):
     committed ncu summary of the kernel (profiles/): its line
     `dram_bytes_per_ray: X` (measured on a smaller capture, scaled by the
     rays of this launch), or None."""
-    p = os.path.join(ROOT, "profiles", f"trace_closest_{layout}_intersect.md")
+    kernel_layout = {"bvh": "bvh2", "qbvh": "bvh4"}[layout]
+    p = os.path.join(ROOT, "profiles", f"trace_closest_{kernel_layout}_intersect.md")
     if os.path.exists(p):
         with open(p) as f:
             for line in f:
