@@ -29,13 +29,17 @@ struct TraversalRay {
     float d[3];
     float inv_min[3];   // 1/d, or 0 where d == 0      (scene.bvh.cpp:124-127)
     float inv_max[3];   // 1/d, or FLT_MAX where d == 0 (scene.bvh.cpp:129-132)
-    uint32_t neg;       // bit c set iff d[c] < 0        (scene.bvh.cpp:134-137)
+    uint32_t neg;       // bit c set iff d[c] < 0        (scene.bvh.cpp:134-137);
+                        // bit 3: finite origin, every d[c] != 0 with a finite 1/d
+                        // (RAY_FINITE_INV)
     float tmin, tmax;
 };
 
+constexpr uint32_t RAY_FINITE_INV = 8u;
+
 __device__ __forceinline__ void setup_ray(TraversalRay& r, const RayIn& in)
 {
-    r.neg = 0;
+    r.neg = RAY_FINITE_INV;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
         r.o[c] = in.o[c];
@@ -45,6 +49,8 @@ __device__ __forceinline__ void setup_ray(TraversalRay& r, const RayIn& in)
         r.inv_min[c] = z ? 0.0f : inv;
         r.inv_max[c] = z ? FLT_MAX : inv;
         r.neg |= (in.d[c] < 0.0f ? 1u : 0u) << c;
+        const float inf = __int_as_float(0x7f800000);
+        if (z || !(fabsf(inv) < inf) || !(fabsf(in.o[c]) < inf)) r.neg &= ~RAY_FINITE_INV;
     }
     r.tmin = in.tmin;
     r.tmax = in.tmax;
@@ -74,6 +80,33 @@ __device__ __forceinline__ bool slab_intrinsic(const TraversalRay& r,
     if (tzmax < tmax) tmax = tzmax;
     t_enter = tmin;
     return tmax > r.tmin;
+}
+
+// The same slab test for a ray with RAY_FINITE_INV and a box with finite
+// lo <= hi on every axis (every binary node's child box). Then inv_min == inv_max,
+// the near/far plane distances of an axis are min/max of its two plane
+// distances (a float subtraction and multiplication round monotonically),
+// no value is NaN, and the reference's pairwise comparison chain fails
+// exactly when max(near) > min(far); its final tmin is max(near). The verdict
+// and t_enter therefore equal slab_intrinsic's (t_enter up to the sign of a
+// zero, which no comparison distinguishes).
+#ifndef LMGPU_TRACE_FAST_SLAB
+#define LMGPU_TRACE_FAST_SLAB 1
+#endif
+__device__ __forceinline__ bool slab_finite(const TraversalRay& r,
+                                            float lox, float hix, float loy, float hiy,
+                                            float loz, float hiz, float& t_enter)
+{
+    const float ax = __fmul_rn(__fsub_rn(lox, r.o[0]), r.inv_min[0]);
+    const float bx = __fmul_rn(__fsub_rn(hix, r.o[0]), r.inv_min[0]);
+    const float ay = __fmul_rn(__fsub_rn(loy, r.o[1]), r.inv_min[1]);
+    const float by = __fmul_rn(__fsub_rn(hiy, r.o[1]), r.inv_min[1]);
+    const float az = __fmul_rn(__fsub_rn(loz, r.o[2]), r.inv_min[2]);
+    const float bz = __fmul_rn(__fsub_rn(hiz, r.o[2]), r.inv_min[2]);
+    const float tn = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fminf(az, bz));
+    const float tf = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
+    t_enter = tn;
+    return tn <= tf && tf > r.tmin;
 }
 
 // TriAccel::Intersect (triaccel.h:100-160) in the reference's order.
@@ -191,8 +224,14 @@ __device__ __forceinline__ bool bvh2_descend(const Bvh2Node* __restrict__ nodes,
         const float4 bx = __ldg(np), by = __ldg(np + 1), bz = __ldg(np + 2);
         const int4 meta = __ldg(reinterpret_cast<const int4*>(np + 3));
         float tl = 0.f, tr = 0.f;
-        const bool pl = slab_intrinsic(r, bx.x, bx.y, by.x, by.y, bz.x, bz.y, tl);
-        const bool pr = slab_intrinsic(r, bx.z, bx.w, by.z, by.w, bz.z, bz.w, tr);
+        bool pl, pr;
+        if (LMGPU_TRACE_FAST_SLAB && (r.neg & RAY_FINITE_INV)) {
+            pl = slab_finite(r, bx.x, bx.y, by.x, by.y, bz.x, bz.y, tl);
+            pr = slab_finite(r, bx.z, bx.w, by.z, by.w, bz.z, bz.w, tr);
+        } else {
+            pl = slab_intrinsic(r, bx.x, bx.y, by.x, by.y, bz.x, bz.y, tl);
+            pr = slab_intrinsic(r, bx.z, bx.w, by.z, by.w, bz.z, bz.w, tr);
+        }
         const bool right_first = (r.neg >> meta.z) & 1u;
         const int32_t near_ref = right_first ? meta.y : meta.x;
         const int32_t far_ref = right_first ? meta.x : meta.y;

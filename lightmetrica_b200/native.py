@@ -1,7 +1,8 @@
 """ctypes binding of the C ABI declared in include/lmgpu.h.
 
-The product path always goes through lightmetrica_b200/_lib/liblmgpu.so;
-there is no CPU fallback. Loading fails loudly if the library is missing.
+The product path always goes through the native library
+(lightmetrica_b200/_lib/liblmgpu.so unless LMGPU_LIBRARY names another
+build); there is no CPU fallback. Loading fails loudly if it is missing.
 """
 from __future__ import annotations
 
@@ -9,7 +10,9 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_lib", "liblmgpu.so")
+# The in-tree build; LMGPU_LIBRARY names another build of the same sources
+# (for example one compiled with different tuning constants).
+LIB_PATH = os.environ.get("LMGPU_LIBRARY") or os.path.join(HERE, "_lib", "liblmgpu.so")
 
 c_int32 = ctypes.c_int32
 c_int64 = ctypes.c_int64
@@ -92,12 +95,12 @@ class RenderStats(ctypes.Structure):
                 ("waves", c_int32), ("max_bounces_run", c_int32), ("device_ms", c_double)]
 
 
-# Every symbol include/lmgpu.h declares, with (restype, argtypes).
 class BatchConfig(ctypes.Structure):
     _fields_ = [("layout", c_int32), ("wave_paths", c_int32), ("shade_blocks_per_sm", c_int32),
                 ("use_graph", c_int32)]
 
 
+# Every symbol include/lmgpu.h declares, with (restype, argtypes).
 SIGNATURES = {
     "lmgpu_abi_version": (c_int32, []),
     "lmgpu_last_error": (ctypes.c_char_p, []),
