@@ -241,6 +241,7 @@ def run_ours(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
     from lightmetrica_b200 import native
+    from lightmetrica_b200.distributed import aggregate_rate, max_over_ranks
     from lightmetrica_b200.scene import Scene, soup_primitives
     from lightmetrica_b200.workloads import random_rays, random_soup, rays_soa
 
@@ -299,12 +300,9 @@ def run_ours(args):
     scene.status(stream.cuda_stream)
     total_ms = t_start.elapsed_time(t_end)
     launch_ms = [a.elapsed_time(b) for a, b in ev]
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t[0])
+    total_ms = max_over_ranks(total_ms, device=dev)
     ms_per_step = total_ms / args.steps
-    value = world * n * args.steps / (total_ms / 1e3) / 1e6
+    value = aggregate_rate(n, args.steps, total_ms, world) / 1e6
 
     # End to end through the host-buffer entry point: pinned AoS rays in, hit
     # arrays out, copies inside the timed region.
@@ -646,6 +644,7 @@ def run_e2e(args, scene, rays, hits, world, dev):
     pinned AoS rays in, hit arrays out, copies inside the timed region."""
     import torch
     from lightmetrica_b200 import native
+    from lightmetrica_b200.distributed import aggregate_rate, max_over_ranks
     L = native.lib()
     n = rays.shape[0]
     rays_pinned = torch.from_numpy(rays).pin_memory()
@@ -664,12 +663,8 @@ def run_e2e(args, scene, rays, hits, world, dev):
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         e2e_once()
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t[0])
-    e2e_value = world * n * e2e_steps / e2e_s / 1e6
+    e2e_s = max_over_ranks(time.perf_counter() - t0, device=dev)
+    e2e_value = aggregate_rate(n, e2e_steps, e2e_s * 1e3, world) / 1e6
     assert np.array_equal(out_id.numpy(), hits["tri_id"].cpu().numpy()), "host and device paths disagree"
     return {"value": round(e2e_value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": n * 32,
             "d2h_bytes_per_step": n * 16, "steps": e2e_steps}

@@ -105,5 +105,10 @@ def create_renderer(impl: str = "pt") -> Renderer:
     return Renderer(impl)
 
 
-def create_scheduler(impl: str = "mt") -> RenderProcessScheduler:
+def create_scheduler(impl: str = "mt"):
+    """"mt" (one GPU: the whole budget in one call) or "mpi" (one process per
+    GPU, sample shards and one film reduce; lightmetrica_b200.distributed)."""
+    if impl == "mpi":
+        from .distributed import MPIRenderProcessScheduler
+        return MPIRenderProcessScheduler(impl)
     return RenderProcessScheduler(impl)

@@ -404,6 +404,22 @@ def oracle_render(prims, technique="pt.mis", spp=16, rr_depth=1, max_path_vertic
     return (film * (W * H / total)).reshape(H, W, 3)
 
 
+def oracle_render_range(prims, sample_begin, sample_end, technique="pt.mis", rr_depth=1, max_path_vertices=-1,
+                        seed=1, sampling="stratified"):
+    """The C restatement's un-rescaled film (W*H*3 float64 sums) of the
+    samples [sample_begin, sample_end) only, one thread."""
+    L = lib()
+    L.orc_render.restype = ctypes.c_int64
+    L.orc_render.argtypes = [ctypes.POINTER(_OrcPtDesc), ctypes.c_void_p]
+    d, keep = _pt_desc(prims, technique, rr_depth, max_path_vertices, seed, sampling, None, None)
+    W, H = prims.camera.film.width, prims.camera.film.height
+    film = np.zeros(W * H * 3)
+    d.sample_begin = int(sample_begin)
+    d.sample_end = int(sample_end)
+    L.orc_render(ctypes.byref(d), film.ctypes.data)
+    return film
+
+
 def oracle_grad(prims, dL_dimage, technique="pt.mis", spp=16, rr_depth=1, max_path_vertices=-1, seed=1,
                 sampling="stratified", threads=None, tri_albedo=None, light_Le=None):
     """FP64 reference gradient of a loss with image gradient dL_dimage

@@ -120,3 +120,24 @@ def test_terrain_image_matches_reference(cuda, golden_dir):
     assert np.isfinite(film).all()
     assert e <= RELMSE_BAR, f"relMSE {e:.3e}"
     np.testing.assert_allclose(film.mean(axis=(0, 1)), ref.mean(axis=(0, 1)), rtol=2e-2)
+
+
+def test_mpi_scheduler_on_one_rank_matches_mt(cuda):
+    """The "mpi" scheduler (sample shards + film reduce) with one process is
+    the "mt" render of the same samples (FP64 shard film vs FP32 film)."""
+    prims = scenes.cornell_box(32, 32, variant="mixed")
+    scene = create_scene("bvh")
+    scene.load(prims)
+    scene.configure({})
+    scene.build()
+    r = create_renderer("pt.mis")
+    r.configure({"rr_depth": 3, "max_path_vertices": 9, "sampler": {"rng_seed": 4}})
+    n = 32 * 32 * 64
+    mpi = create_scheduler("mpi")
+    mpi.configure({"num_samples": n})
+    got = mpi.render(r, scene)
+    assert mpi.last_shard == (0, n)
+    mt = create_scheduler("mt")
+    mt.configure({"num_samples": n})
+    np.testing.assert_allclose(got, mt.render(r, scene), rtol=1e-4, atol=1e-6)
+    scene.close()
