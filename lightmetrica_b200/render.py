@@ -74,6 +74,8 @@ class RenderProcessScheduler:
         self.num_samples = 1
         self.film_fp64 = False
         self.wave_paths = 0
+        self.progress_image_interval = -1.0
+        self.progress_images = []
         self.last_stats = None
 
     def configure(self, node: Optional[dict] = None, assets=None) -> bool:
@@ -81,6 +83,7 @@ class RenderProcessScheduler:
         self.num_samples = int(node.get("num_samples", 1))
         self.film_fp64 = bool(node.get("film_fp64", False))
         self.wave_paths = int(node.get("wave_paths", 0))
+        self.progress_image_interval = float(node.get("progress_image_interval", -1.0))
         if self.num_samples <= 0:
             raise ValueError("num_samples must be positive")
         return True
@@ -91,12 +94,56 @@ class RenderProcessScheduler:
         cam = scene.main_camera()
         if cam is None or cam.film is None:
             raise RuntimeError("scene has no main camera / film")
+        if self.progress_image_interval > 0.0:
+            return self._render_with_progress(renderer, scene, cam)
         film = np.zeros((cam.film.height, cam.film.width, 3), np.float32)
         p = renderer.params(self.num_samples, film_fp64=self.film_fp64, wave_paths=self.wave_paths)
         st = N.RenderStats()
         N.check(N.lib().lmgpu_render(scene.handle, ctypes.byref(p), film.ctypes.data, ctypes.byref(st)))
         self.last_stats = {"rays_traced": st.rays_traced, "shadow_rays": st.shadow_rays, "paths": st.paths,
                            "waves": st.waves, "max_bounces_run": st.max_bounces_run, "device_ms": st.device_ms}
+        cam.film.data = film
+        return film
+
+
+    def _render_with_progress(self, renderer, scene, cam) -> np.ndarray:
+        """progress_image_interval > 0 (sched.mt.cpp:197-228): the budget is
+        rendered in chunks into one device film; whenever more than the
+        interval (seconds) has passed since the last image, the film so far
+        is rescaled by W*H / processed samples and saved as
+        progress.<renderer>/%010d(.hdr|.exr)."""
+        import os
+        import time
+        import torch
+        W, H = cam.film.width, cam.film.height
+        dev_film = torch.zeros(W * H * 3, dtype=torch.float64 if self.film_fp64 else torch.float32, device="cuda")
+        stream = torch.cuda.current_stream().cuda_stream
+        chunk = max(W * H, self.num_samples // 64)
+        done, count = 0, 0
+        last = time.perf_counter()
+        out_dir = "progress." + renderer.type()
+        self.progress_images = []
+        totals = {"rays_traced": 0, "shadow_rays": 0, "paths": 0, "waves": 0, "max_bounces_run": 0, "device_ms": 0.0}
+        while done < self.num_samples:
+            n = min(chunk, self.num_samples - done)
+            p = renderer.params(n, sample_offset=done, film_fp64=self.film_fp64, wave_paths=self.wave_paths)
+            st = N.RenderStats()
+            N.check(N.lib().lmgpu_render_device(scene.handle, ctypes.byref(p), ctypes.c_void_p(dev_film.data_ptr()),
+                                                ctypes.c_void_p(stream), ctypes.byref(st)))
+            for k in ("rays_traced", "shadow_rays", "paths", "waves", "device_ms"):
+                totals[k] += getattr(st, k)
+            totals["max_bounces_run"] = max(totals["max_bounces_run"], st.max_bounces_run)
+            done += n
+            now = time.perf_counter()
+            if now - last > self.progress_image_interval and done < self.num_samples:
+                count += 1
+                img = (dev_film.double().cpu().numpy() * (W * H / done)).astype(np.float32).reshape(H, W, 3)
+                from .film_io import save_film
+                self.progress_images.append(save_film(img, os.path.join(out_dir, "%010d" % count),
+                                                      cam.film.image_type))
+                last = now
+        film = (dev_film.double().cpu().numpy() * (W * H / self.num_samples)).astype(np.float32).reshape(H, W, 3)
+        self.last_stats = totals
         cam.film.data = film
         return film
 

@@ -75,11 +75,21 @@ class HDRBitmapFilm:
     width: int
     height: int
     data: Optional[np.ndarray] = None
+    image_type: str = "radiancehdr"        # or "openexr" (hdrfilm.cpp:88-107)
 
     def internal_data(self) -> np.ndarray:
         if self.data is None:
             self.data = np.zeros((self.height, self.width, 3), np.float32)
         return self.data
+
+    def rescale_and_save(self, path: str, weight: float = 1.0) -> str:
+        """HDRBitmapFilm::RescaleAndSave (hdrfilm.cpp:199-304); returns the
+        path written (see film_io for the naming rules)."""
+        from .film_io import save_film
+        return save_film(self.internal_data(), path, self.image_type, weight)
+
+    def save(self, path: str) -> str:
+        return self.rescale_and_save(path, 1.0)
 
 
 @dataclass

@@ -23,6 +23,8 @@ Fixtures:
   terrain_ref_mis_96x54.npz
                            the reference's double-precision pt.mis image of
                            scenes.terrain_spheres at 96 x 54 (16384 spp)
+  ref_scene_literals.json  the XML scene literals of the reference's Primitives
+                           and BPT tests (inputs of tests/test_sceneio.py)
 Each fixture stores the inputs with the reference outputs for every scene
 type the reference builds here (bvh, qbvh, naive).
 """
@@ -170,8 +172,32 @@ def terrain_image(spp: int = 16384):
     print("wrote terrain image", f"{spp} spp {secs:.1f} s", film.mean(axis=(0, 1)))
 
 
+def scene_literals(reference_root: str = "/root/reference"):
+    """The XML scene literals of the reference's own Primitives and BPT tests
+    (test.primitives.cpp: SceneNode_Success, _WithTransformByMatrix,
+    _WithTransform; test.bpt.mis.cpp: SceneFile), extracted verbatim as test
+    inputs; the expected values live in tests/test_sceneio.py with the
+    reference assertions they restate."""
+    import json
+    import re
+    out = {}
+    for fname, names in (("test.primitives.cpp", ("SceneNode_Success", "SceneNode_Success_WithTransformByMatrix",
+                                                   "SceneNode_Success_WithTransform")),
+                         ("test.bpt.mis.cpp", ("SceneFile",))):
+        src = open(os.path.join(reference_root, "src", "lightmetrica.test", fname)).read()
+        for name in names:
+            m = re.search(r"const std::string " + name + r" = LM_TEST_MULTILINE_LITERAL\((.*?)\n\t\);", src, re.S)
+            if not m:
+                raise RuntimeError(f"literal {name} not found in {fname}")
+            out[f"{fname}:{name}"] = m.group(1).strip()
+    with open(os.path.join(OUT, "ref_scene_literals.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    print("wrote", len(out), "scene literals")
+
+
 if __name__ == "__main__":
     main()
+    scene_literals()
     if oracle.ref_available("d"):
         images()
         terrain_image()
