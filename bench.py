@@ -405,6 +405,21 @@ def render_section(args, dev, cpu_baseline):
     ms = sum(x[0] for x in runs) / len(runs)
     rays = sum(x[1] for x in runs) / len(runs)
     shadow = sum(x[2] for x in runs) / len(runs)
+    # The batch path with this one scene: autotuned configuration (untimed),
+    # waves replayed from a captured CUDA graph, no host synchronisation.
+    from lightmetrica_b200.batch import SceneBatch
+    batch = SceneBatch([scene])
+    t0 = time.perf_counter()
+    tuned = batch.autotune([r], [n], sample_fraction=1.0 / 8)
+    tune_s = time.perf_counter() - t0
+    batch.render_device([r], [n], [film])                       # warm-up (graph capture)
+    bruns = []
+    for _ in range(max(1, args.render_frames)):
+        batch.render_device([r], [n], [film])
+        bruns.append((batch.last_stats["device_ms"], batch.last_stats["rays_traced"]))
+    batch.close()
+    b_ms = sum(x[0] for x in bruns) / len(bruns)
+    b_rays = sum(x[1] for x in bruns) / len(bruns)
     # End to end through the scheduler (host film out, rescaled).
     sched = create_scheduler("mt")
     sched.configure({"num_samples": n})
@@ -425,6 +440,9 @@ def render_section(args, dev, cpu_baseline):
                     f"{W}x{H}, {S} spp, pt.mis, max depth 16, Russian roulette after depth 4",
         "Mrays_per_s": round(rays / (ms / 1e3) / 1e6, 1),
         "spp_per_s": round(S / (ms / 1e3), 2),
+        "batched": {"Mrays_per_s": round(b_rays / (b_ms / 1e3) / 1e6, 1), "spp_per_s": round(S / (b_ms / 1e3), 2),
+                    "ms_per_frame": round(b_ms, 2), "autotuned": tuned, "autotune_seconds": round(tune_s, 2),
+                    "note": "the multi-scene batch path with this one scene: same samples, same paths"},
         "Msamples_per_s": round(n / (ms / 1e3) / 1e6, 2),
         "ms_per_frame": round(ms, 2), "rays_per_frame": int(rays), "shadow_rays_per_frame": int(shadow),
         "frames_timed": len(runs), "waves_per_frame": runs[0][3],
