@@ -261,12 +261,20 @@ __global__ void __launch_bounds__(128) k_pt_init(const Ctx ctx, const PathState 
 // scene table each ray is traced in its own path's scene.
 // Both path-tracer queues refill traversal lanes 24 at a time (measured on
 // the 1080p terrain: a few percent faster than 8).
-constexpr int PATH_QUEUE_REFILL_MIN = 24;
+#ifndef LMGPU_PT_REFILL_MIN
+#define LMGPU_PT_REFILL_MIN 24
+#endif
+#ifndef LMGPU_PT_EXIT_BELOW
+#define LMGPU_PT_EXIT_BELOW 24
+#endif
+constexpr int PATH_QUEUE_REFILL_MIN = LMGPU_PT_REFILL_MIN;
+constexpr int PATH_QUEUE_EXIT_BELOW = LMGPU_PT_EXIT_BELOW;
 
 template <bool TABLE>
 struct PathRayIO {
     static constexpr bool PER_RAY_SCENE = TABLE;
     static constexpr int REFILL_MIN = PATH_QUEUE_REFILL_MIN;
+    static constexpr int EXIT_BELOW = PATH_QUEUE_EXIT_BELOW;
     const int32_t* queue;
     const uint32_t* count_ptr;
     const float4* ray_o;
@@ -299,6 +307,7 @@ template <class Ctx>
 struct ShadowIO {
     static constexpr bool PER_RAY_SCENE = Ctx::TABLE;
     static constexpr int REFILL_MIN = PATH_QUEUE_REFILL_MIN;
+    static constexpr int EXIT_BELOW = PATH_QUEUE_EXIT_BELOW;
     const uint32_t* count_ptr;
     const float4* sh_o;
     const float4* sh_d;

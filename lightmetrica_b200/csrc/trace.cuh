@@ -183,12 +183,37 @@ struct TravState {
     int sp;
 };
 
+// Traversal stack storage: a per-thread array (local memory), or a split
+// stack whose first S entries live in shared memory ([S][128] per block of
+// 128 threads: lanes hit distinct banks) and the rest in local memory, so
+// the stack's bottom no longer competes with tree nodes for L1.
+__device__ __forceinline__ void stack_put(int2* s, int i, int2 v) { s[i] = v; }
+__device__ __forceinline__ int2 stack_get(const int2* s, int i) { return s[i]; }
+
+template <int S>
+struct SplitStack {
+    int2 (*sh)[128];
+    int2* local;
+};
+template <int S>
+__device__ __forceinline__ void stack_put(const SplitStack<S>& s, int i, int2 v)
+{
+    if (i < S) s.sh[i][threadIdx.x] = v;
+    else s.local[i - S] = v;
+}
+template <int S>
+__device__ __forceinline__ int2 stack_get(const SplitStack<S>& s, int i)
+{
+    return i < S ? s.sh[i][threadIdx.x] : s.local[i - S];
+}
+
 // Pops the next deferred child whose box is still entered before maxT
 // (the reference's far-child test, evaluated with the current maxT).
-__device__ __forceinline__ void pop_next(TravState& ts, const int2* stack, const TraversalRay& r, TraceStats* st)
+template <class Stack>
+__device__ __forceinline__ void pop_next(TravState& ts, Stack stack, const TraversalRay& r, TraceStats* st)
 {
     while (ts.sp > 0) {
-        const int2 e = stack[--ts.sp];
+        const int2 e = stack_get(stack, --ts.sp);
         if (st) st->nodes++;
         if (__int_as_float(e.y) < r.tmax) { ts.ref = e.x; return; }
     }
@@ -211,8 +236,8 @@ __device__ __forceinline__ void trav_begin(TravState& ts, int32_t root_ref, cons
 // `may_exit`, it also returns (state intact, at an internal node) once fewer
 // than EXIT_BELOW lanes of the warp are still descending, after at least one
 // step: the caller resumes it later, so the ray's walk is unchanged.
-template <int EXIT_BELOW = 0>
-__device__ __forceinline__ bool bvh2_descend(const Bvh2Node* __restrict__ nodes, TravState& ts, int2* stack,
+template <int EXIT_BELOW = 0, class Stack>
+__device__ __forceinline__ bool bvh2_descend(const Bvh2Node* __restrict__ nodes, TravState& ts, Stack stack,
                                              int stack_cap, const TraversalRay& r, TraceStats* st,
                                              bool may_exit = false)
 {
@@ -243,7 +268,7 @@ __device__ __forceinline__ bool bvh2_descend(const Bvh2Node* __restrict__ nodes,
         if (near_pass && near_t < r.tmax) {
             if (far_pass) {
                 if (ts.sp >= stack_cap) return false;
-                stack[ts.sp++] = make_int2(far_ref, __float_as_int(far_t));
+                stack_put(stack, ts.sp++, make_int2(far_ref, __float_as_int(far_t)));
             } else if (st) {
                 st->nodes++;                         // far child's (failing) test
             }

@@ -15,8 +15,8 @@ namespace lmgpu {
 
 // 4-wide nodes: descends until the state reaches a leaf or finishes.
 // Returns false on stack overflow. EXIT_BELOW / may_exit as in bvh2_descend.
-template <int EXIT_BELOW = 0>
-__device__ __forceinline__ bool bvh4_descend(const Bvh4Node* __restrict__ nodes, TravState& ts, int2* stack,
+template <int EXIT_BELOW = 0, class Stack>
+__device__ __forceinline__ bool bvh4_descend(const Bvh4Node* __restrict__ nodes, TravState& ts, Stack stack,
                                              int stack_cap, const TraversalRay& r, TraceStats* st,
                                              bool may_exit = false)
 {
@@ -76,7 +76,7 @@ __device__ __forceinline__ bool bvh4_descend(const Bvh4Node* __restrict__ nodes,
             if (ts.sp + (np_ - 1 - first) > stack_cap) return false;
 #pragma unroll
             for (int j = 3; j >= 0; j--)
-                if (j > first && j < np_) stack[ts.sp++] = make_int2(refs[j], __float_as_int(ts4[j]));
+                if (j > first && j < np_) stack_put(stack, ts.sp++, make_int2(refs[j], __float_as_int(ts4[j])));
             ts.ref = refs[first];
             continue;
         }

@@ -22,7 +22,10 @@ namespace lmgpu {
 #define LMGPU_TRACE_EXIT_BELOW 24     // pause a descent when fewer lanes descend (0: never)
 #endif
 #ifndef LMGPU_TRACE_MIN_BLOCKS
-#define LMGPU_TRACE_MIN_BLOCKS 1      // minimum resident blocks of 128 threads per SM
+#define LMGPU_TRACE_MIN_BLOCKS 10     // minimum resident blocks of 128 threads per SM (48 registers)
+#endif
+#ifndef LMGPU_TRACE_SHARED_STACK
+#define LMGPU_TRACE_SHARED_STACK 12   // stack entries per lane kept in shared memory (0: none)
 #endif
 
 // I/O policies whose rays each belong to their own scene (a multi-scene
@@ -40,6 +43,12 @@ struct refill_min : std::integral_constant<int, LMGPU_TRACE_REFILL_MIN> {};
 template <class IO>
 struct refill_min<IO, std::void_t<decltype(IO::REFILL_MIN)>> : std::integral_constant<int, IO::REFILL_MIN> {};
 
+// Pause threshold of a descent: an I/O policy may declare EXIT_BELOW.
+template <class IO, class = void>
+struct exit_below : std::integral_constant<int, LMGPU_TRACE_EXIT_BELOW> {};
+template <class IO>
+struct exit_below<IO, std::void_t<decltype(IO::EXIT_BELOW)>> : std::integral_constant<int, IO::EXIT_BELOW> {};
+
 // Node and triangle arrays of the scene a lane is tracing.
 struct LaneScene {
     const Bvh2Node* bvh2;
@@ -48,13 +57,12 @@ struct LaneScene {
 };
 
 
-template <int LAYOUT>
-__device__ __forceinline__ bool descend(const LaneScene& s, TravState& ts, int2* stack, int cap, const TraversalRay& r,
-                                        bool may_exit)
+template <int LAYOUT, int EXIT, class Stack>
+__device__ __forceinline__ bool descend(const LaneScene& s, TravState& ts, Stack stack, int cap,
+                                        const TraversalRay& r, bool may_exit)
 {
-    if (LAYOUT == LMGPU_LAYOUT_BVH2)
-        return bvh2_descend<LMGPU_TRACE_EXIT_BELOW>(s.bvh2, ts, stack, cap, r, nullptr, may_exit);
-    return bvh4_descend<LMGPU_TRACE_EXIT_BELOW>(s.bvh4, ts, stack, cap, r, nullptr, may_exit);
+    if (LAYOUT == LMGPU_LAYOUT_BVH2) return bvh2_descend<EXIT>(s.bvh2, ts, stack, cap, r, nullptr, may_exit);
+    return bvh4_descend<EXIT>(s.bvh4, ts, stack, cap, r, nullptr, may_exit);
 }
 
 // Persistent traversal with per-lane ray replacement: a warp keeps tracing
@@ -75,7 +83,14 @@ __global__ void __launch_bounds__(128, LMGPU_TRACE_MIN_BLOCKS) k_trace_persisten
                                                           unsigned long long* next_ray)
 {
     constexpr unsigned FULL = 0xffffffffu;
+#if LMGPU_TRACE_SHARED_STACK > 0
+    constexpr int SH = LMGPU_TRACE_SHARED_STACK < STACK ? LMGPU_TRACE_SHARED_STACK : STACK;
+    __shared__ int2 stack_sh[SH][128];
+    int2 stack_local[STACK > SH ? STACK - SH : 1];
+    const SplitStack<SH> stack{ stack_sh, stack_local };
+#else
     int2 stack[STACK];
+#endif
     const int64_t n = io.count();
     const unsigned lane = threadIdx.x & 31u;
     const int32_t root = LAYOUT == LMGPU_LAYOUT_BVH2 ? s.root_ref : s.root_ref4;
@@ -119,7 +134,7 @@ __global__ void __launch_bounds__(128, LMGPU_TRACE_MIN_BLOCKS) k_trace_persisten
             break;
         }
         if (ts.ref != REF_DONE) {
-            if (!descend<LAYOUT>(ls, ts, stack, STACK, r, !exhausted)) {
+            if (!descend<LAYOUT, exit_below<IO>::value>(ls, ts, stack, STACK, r, !exhausted)) {
                 atomicOr(status, STATUS_STACK_OVERFLOW);
                 h.tri = -1;
                 ts.ref = REF_DONE;
