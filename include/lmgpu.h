@@ -217,7 +217,11 @@ int lmgpu_render(LmgpuScene* scene, const LmgpuRenderParams* params,
 
 /* Device variant: accumulates un-rescaled contributions into a DEVICE film
  * (float, or double when film_fp64) on `stream`; the caller rescales by
- * W*H/num_samples. No host synchronisation. */
+ * W*H/num_samples. The call returns once the render's device work is done
+ * (it reads each bounce's queue sizes back to size the next launch). Waves
+ * hold `wave_paths` paths (0 = 2^24, fewer if device memory is short) in a
+ * workspace of about 176 bytes per path that is shared by all scenes of the
+ * device and kept until exit; calls on one device take turns. */
 int lmgpu_render_device(LmgpuScene* scene, const LmgpuRenderParams* params,
                         void* film_device, void* stream, LmgpuRenderStats* stats);
 
@@ -289,7 +293,8 @@ typedef struct LmgpuBatchConfig {
 
 /* The scenes (built with a BVH layout, on the current device) must outlive
  * the batch; a scene may appear more than once. Default configuration:
- * BVH2, 2^21 paths per wave, 8 shading blocks per SM, graphs on. */
+ * BVH2, 2^24 paths per wave (about 3 GB of wave state), 16 shading blocks
+ * per SM, graphs on; a device short of memory gets smaller waves. */
 int lmgpu_batch_create(LmgpuScene* const* scenes, int32_t num_scenes, LmgpuBatch** out);
 int lmgpu_batch_destroy(LmgpuBatch* batch);
 int lmgpu_batch_get_config(const LmgpuBatch* batch, LmgpuBatchConfig* config);

@@ -503,7 +503,6 @@ int lmgpu_scene_destroy(LmgpuScene* scene)
     if (!scene) return LMGPU_OK;
     if (scene->pipe.ready)
         for (int k = 0; k < 2; k++) cudaStreamDestroy(scene->pipe.stream[k]);
-    release_render_workspace(scene);
     for (void* p : scene->allocations) cudaFree(p);
     delete scene;
     return LMGPU_OK;

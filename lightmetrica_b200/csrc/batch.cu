@@ -53,7 +53,7 @@ struct LmgpuBatch {
     int device = 0;
     int sms = 148;
     std::vector<LmgpuScene*> scenes;
-    LmgpuBatchConfig cfg{ LMGPU_LAYOUT_BVH2, 1 << 21, 8, 1 };
+    LmgpuBatchConfig cfg{ LMGPU_LAYOUT_BVH2, 1 << 24, 16, 1 };
 
     BatchEntry* d_table = nullptr;
     int64_t* d_begins = nullptr;
@@ -389,7 +389,7 @@ int check_config(const LmgpuBatchConfig& c)
 {
     if (c.layout != LMGPU_LAYOUT_BVH2 && c.layout != LMGPU_LAYOUT_BVH4)
         return fail(LMGPU_ERR_INVALID, "batch layout must be LMGPU_LAYOUT_BVH2 or LMGPU_LAYOUT_BVH4");
-    if (c.wave_paths < 1024 || c.wave_paths > (1 << 24)) return fail(LMGPU_ERR_INVALID, "wave_paths must be in [1024, 2^24]");
+    if (c.wave_paths < 1024 || c.wave_paths > (1 << 26)) return fail(LMGPU_ERR_INVALID, "wave_paths must be in [1024, 2^26]");
     if (c.shade_blocks_per_sm < 1 || c.shade_blocks_per_sm > 64) return fail(LMGPU_ERR_INVALID, "shade_blocks_per_sm must be in [1, 64]");
     return LMGPU_OK;
 }
@@ -405,8 +405,14 @@ int batch_render(LmgpuBatch* b, const LmgpuRenderParams* params, void* const* fi
     int cur = 0;
     LMGPU_CUDA_TRY(cudaGetDevice(&cur));
     if (cur != b->device) return fail(LMGPU_ERR_INVALID, "batch used on another device than it was created on");
-    const int64_t P = std::min<int64_t>(b->cfg.wave_paths, pl.total);
-    if ((rc = ensure_batch_workspace(b, std::max<int64_t>(P, b->ws_capacity))) != LMGPU_OK) return rc;
+    int64_t P = std::min<int64_t>(b->cfg.wave_paths, pl.total);
+    rc = ensure_batch_workspace(b, std::max<int64_t>(P, b->ws_capacity));
+    // A device short of memory gets smaller waves (the configuration stays).
+    while (rc == LMGPU_ERR_OOM && P > (int64_t(1) << 20)) {
+        P /= 2;
+        rc = ensure_batch_workspace(b, P);
+    }
+    if (rc != LMGPU_OK) return rc;
     if ((rc = upload_table(b, params, films, s)) != LMGPU_OK) return rc;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (stats) {
@@ -560,6 +566,7 @@ int lmgpu_batch_autotune(LmgpuBatch* b, const LmgpuRenderParams* params, double 
     auto trial = [&](const LmgpuBatchConfig& c, double& ms) -> int {
         int r = check_config(c);
         if (r != LMGPU_OK) return r;
+        ms = 1e30;
         b->cfg = c;
         LmgpuRenderStats st;
         if ((r = batch_render(b, p.data(), films.data(), s, &st)) != LMGPU_OK) return r;   // warm-up (capture)
@@ -577,7 +584,7 @@ int lmgpu_batch_autotune(LmgpuBatch* b, const LmgpuRenderParams* params, double 
     rc = trial(best, best_t);
     // Coordinate descent: layout, then wave size, then shading grid.
     const int layouts[] = { LMGPU_LAYOUT_BVH2, LMGPU_LAYOUT_BVH4 };
-    const int waves[] = { 1 << 19, 1 << 20, 1 << 21, 1 << 22 };
+    const int waves[] = { 1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25 };
     const int grids[] = { 4, 8, 16 };
     for (int l : layouts) {
         if (rc != LMGPU_OK || l == best.layout) continue;

@@ -30,7 +30,6 @@ struct LmgpuScene {
     unsigned long long* d_work = nullptr;
     std::atomic<uint64_t> work_slot{0};
     HostPipeline pipe;
-    void* render_ws = nullptr;        // path-tracer wave workspace (pathtrace.cu)
     // Host copies needed by host-side helpers (light selection tables etc.)
     std::vector<float> bounds_min, bounds_max;
 };
@@ -50,9 +49,6 @@ constexpr int32_t STATUS_TIMEOUT = 4;
 int64_t workspace_paths_for_bytes(size_t bytes);
 int render_device_preallocated(LmgpuScene* sc, const LmgpuRenderParams& p, void* film, cudaStream_t stream,
                                void* ws_mem, size_t ws_bytes, uint32_t* host_counts);
-
-// Frees the path tracer's cached workspace of a scene.
-void release_render_workspace(LmgpuScene* sc);
 
 // Reads and clears the device status word; maps it to an LMGPU status.
 int consume_status(LmgpuScene* s, cudaStream_t stream);

@@ -142,7 +142,7 @@ def test_batch_autotune_keeps_results(cuda):
     batch = SceneBatch(built)
     cfg = batch.autotune([r for _, r, _ in items], [n for _, _, n in items], sample_fraction=0.25)
     assert cfg["layout"] in ("bvh", "qbvh") and cfg["trial_ms"] > 0
-    assert cfg["wave_paths"] in (1 << 19, 1 << 20, 1 << 21, 1 << 22)
+    assert cfg["wave_paths"] in (1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25)
     assert_same(batch_films(batch, items), want)
     batch.close()
 
