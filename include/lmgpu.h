@@ -284,17 +284,26 @@ int lmgpu_adjoint_backward(LmgpuScene* scene, const LmgpuRenderParams* params,
  * with the same parameters (same random numbers, same paths). */
 typedef struct LmgpuBatch LmgpuBatch;
 
+enum {
+    LMGPU_BATCH_WAVES = 0,   /* fixed waves: each wave's paths run to the end before the next wave */
+    LMGPU_BATCH_STREAM = 1   /* path regeneration: finished paths' slots take new paths every
+                                iteration, so the queues stay full until the samples run out */
+};
+
 typedef struct LmgpuBatchConfig {
     int32_t layout;               /* LMGPU_LAYOUT_BVH2 or LMGPU_LAYOUT_BVH4 for every scene */
-    int32_t wave_paths;           /* paths per wave: the capacity of the ray and shadow queues */
+    int32_t wave_paths;           /* paths in flight: the capacity of the ray and shadow queues */
     int32_t shade_blocks_per_sm;  /* grid of the shading kernel (blocks of 128 threads per SM) */
-    int32_t use_graph;            /* 1: waves replay a captured CUDA graph; 0: direct launches */
+    int32_t use_graph;            /* 1: replay a captured CUDA graph (a wave, or two stream
+                                     iterations); 0: direct launches */
+    int32_t mode;                 /* LMGPU_BATCH_STREAM (default) or LMGPU_BATCH_WAVES */
 } LmgpuBatchConfig;
 
 /* The scenes (built with a BVH layout, on the current device) must outlive
  * the batch; a scene may appear more than once. Default configuration:
- * BVH2, 2^24 paths per wave (about 3 GB of wave state), 16 shading blocks
- * per SM, graphs on; a device short of memory gets smaller waves. */
+ * BVH2, 2^24 paths in flight (about 3 GB of path state), 16 shading blocks
+ * per SM, graphs on, path regeneration; a device short of memory gets
+ * fewer paths in flight. */
 int lmgpu_batch_create(LmgpuScene* const* scenes, int32_t num_scenes, LmgpuBatch** out);
 int lmgpu_batch_destroy(LmgpuBatch* batch);
 int lmgpu_batch_get_config(const LmgpuBatch* batch, LmgpuBatchConfig* config);
@@ -310,8 +319,8 @@ int lmgpu_batch_render_device(LmgpuBatch* batch, const LmgpuRenderParams* params
                               void* const* films_device, void* stream, LmgpuRenderStats* stats);
 
 /* Autotuner: renders the batch with each scene's sample count scaled by
- * `sample_fraction` (0 < f <= 1) under candidate configurations (BVH
- * layout, wave size, shading grid), coordinate by coordinate, keeps the
+ * `sample_fraction` (0 < f <= 1) under candidate configurations (mode, BVH
+ * layout, paths in flight, shading grid), coordinate by coordinate, keeps the
  * fastest, stores it as the batch's configuration and returns it with its
  * device time in ms. Films are scratch memory of the tuner; synchronises. */
 int lmgpu_batch_autotune(LmgpuBatch* batch, const LmgpuRenderParams* params, double sample_fraction,

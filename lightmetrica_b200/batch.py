@@ -9,8 +9,9 @@ sched.mt.cpp:93-266).
 Each scene keeps its own camera, film, renderer parameters (technique shared
 by the batch) and sample count, and renders exactly the samples it would
 render alone through RenderProcessScheduler.render: same random numbers,
-same paths. All scenes' paths run in shared waves whose kernel sequence is
-replayed from a captured CUDA graph.
+same paths. All scenes' paths share one pool of path slots ("stream" mode:
+finished paths' slots take new paths every iteration) or fixed waves
+("waves"), and the kernel sequence is replayed from a captured CUDA graph.
 """
 from __future__ import annotations
 
@@ -42,10 +43,12 @@ class SceneBatch:
         c = N.BatchConfig()
         N.check(N.lib().lmgpu_batch_get_config(self.handle, ctypes.byref(c)))
         return {"layout": {v: k for k, v in LAYOUTS.items()}[c.layout], "wave_paths": c.wave_paths,
-                "shade_blocks_per_sm": c.shade_blocks_per_sm, "use_graph": bool(c.use_graph)}
+                "shade_blocks_per_sm": c.shade_blocks_per_sm, "use_graph": bool(c.use_graph),
+                "mode": {N.BATCH_WAVES: "waves", N.BATCH_STREAM: "stream"}[c.mode]}
 
     def configure(self, layout: str | None = None, wave_paths: int | None = None,
-                  shade_blocks_per_sm: int | None = None, use_graph: bool | None = None) -> None:
+                  shade_blocks_per_sm: int | None = None, use_graph: bool | None = None,
+                  mode: str | None = None) -> None:
         c = N.BatchConfig()
         N.check(N.lib().lmgpu_batch_get_config(self.handle, ctypes.byref(c)))
         if layout is not None:
@@ -58,6 +61,10 @@ class SceneBatch:
             c.shade_blocks_per_sm = int(shade_blocks_per_sm)
         if use_graph is not None:
             c.use_graph = 1 if use_graph else 0
+        if mode is not None:
+            if mode not in ("waves", "stream"):
+                raise ValueError("mode must be 'waves' or 'stream'")
+            c.mode = N.BATCH_WAVES if mode == "waves" else N.BATCH_STREAM
         N.check(N.lib().lmgpu_batch_set_config(self.handle, ctypes.byref(c)))
 
     # ------------------------------------------------------------ render --

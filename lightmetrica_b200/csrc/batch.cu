@@ -12,6 +12,14 @@
 // launched once per wave with no host synchronisation. Scenes whose depth is
 // unbounded (max_path_vertices = -1) finish their tail bounces with direct
 // launches after the graph.
+//
+// Stream mode (the default) regenerates paths instead: the path slots form
+// one pool, every iteration retires the paths that finished (splat, free the
+// slot) and starts new camera paths in the free slots, so the ray queues
+// stay full until the samples run out and only the batch's last paths run
+// a latency-bound tail. Two iterations (both queue parities) are one
+// captured graph, launched until a device-side flag reports that every
+// sample has started and every slot is free.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
@@ -30,20 +38,25 @@ namespace {
 constexpr int WORK_SLOTS = 160;            // traversal launches per wave: 2 per bounce + 1
 constexpr int GRAPH_BOUNCES_UNBOUNDED = 24;
 constexpr int MAX_BOUNDED_BOUNCES = 64;
-constexpr size_t BYTES_PER_PATH = 16 * 10 + 8 + 4 * 2 + 4;   // path state + scene index
+// path state + scene index + sample index, depth, free list, retire queue;
+// the shadow arrays hold 2 entries per path (in stream mode a new path's
+// camera-vertex shadow ray and its first bounce's share one shadow pass).
+constexpr size_t BYTES_PER_PATH = 16 * 10 + 16 * 3 + 8 + 4 * 2 + 4 + 8 + 4 + 4 + 4;
+constexpr int STREAM_CHECK_EVERY = 8;      // graph launches between checks of the done flag
 
 // Device totals of a render: [0] closest-hit rays, [1] shadow rays,
 // [2] deepest bounce with a live ray.
 constexpr int NSTATS = 4;
 
 struct GraphKey {
-    int tech = -1, fp64 = -1, layout = -1, stack = -1, bounces = -1, bounded = -1, shade_blocks = -1;
+    int tech = -1, fp64 = -1, layout = -1, stack = -1, bounces = -1, bounded = -1, shade_blocks = -1, mode = -1;
     int64_t paths = -1;
     int num_scenes = -1;
     bool operator==(const GraphKey& o) const
     {
         return tech == o.tech && fp64 == o.fp64 && layout == o.layout && stack == o.stack && bounces == o.bounces &&
-               bounded == o.bounded && shade_blocks == o.shade_blocks && paths == o.paths && num_scenes == o.num_scenes;
+               bounded == o.bounded && shade_blocks == o.shade_blocks && paths == o.paths && num_scenes == o.num_scenes &&
+               mode == o.mode;
     }
 };
 
@@ -53,11 +66,13 @@ struct LmgpuBatch {
     int device = 0;
     int sms = 148;
     std::vector<LmgpuScene*> scenes;
-    LmgpuBatchConfig cfg{ LMGPU_LAYOUT_BVH2, 1 << 24, 16, 1 };
+    LmgpuBatchConfig cfg{ LMGPU_LAYOUT_BVH2, 1 << 24, 16, 1, LMGPU_BATCH_STREAM };
 
     BatchEntry* d_table = nullptr;
     int64_t* d_begins = nullptr;
     WaveCtl* d_wave = nullptr;
+    StreamCtl* d_ctl = nullptr;
+    int64_t* h_done = nullptr;              // pinned: StreamCtl::done and ::iterations
     unsigned long long* d_stats = nullptr;
     unsigned long long* d_work = nullptr;
     int32_t* d_status = nullptr;
@@ -120,6 +135,52 @@ __global__ void k_wave_end(WaveCtl* wave, uint32_t* counters, unsigned long long
     wave->count = left <= 0 ? 0 : (left < wave->step ? left : wave->step);
 }
 
+// Stream mode: all slots free, nothing started.
+__global__ void k_stream_setup(StreamCtl* ctl, int64_t total, int64_t capacity, int32_t* free_slots, uint32_t* counters,
+                               unsigned long long* stats)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int64_t i = t; i < capacity; i += (int64_t)gridDim.x * blockDim.x) free_slots[i] = (int32_t)i;
+    if (t == 0) {
+        ctl->next = 0;
+        ctl->total = total;
+        ctl->free_count = capacity;
+        ctl->n_new = 0;
+        ctl->free_base = 0;
+        ctl->g0 = 0;
+        ctl->capacity = capacity;
+        ctl->iterations = 0;
+        ctl->done = 0;
+        for (int i = 0; i < 4; i++) counters[i] = 0;
+        for (int i = 0; i < NSTATS; i++) stats[i] = 0;
+    }
+}
+
+// Start of a stream iteration with input queue q: tally the previous
+// iteration (it traced queue 1 - q and shaded into q), return its retired
+// slots, then start min(free slots, samples left) new paths.
+__global__ void k_stream_plan(StreamCtl* ctl, uint32_t* counters, int q, unsigned long long* stats,
+                              unsigned long long* work)
+{
+    stats[0] += counters[1 - q];
+    stats[1] += counters[2];
+    ctl->free_count += counters[3];
+    counters[1 - q] = 0;
+    counters[2] = 0;
+    counters[3] = 0;
+    const int64_t left = ctl->total - ctl->next;
+    const int64_t n = left < ctl->free_count ? left : ctl->free_count;
+    ctl->done = (left <= 0 && ctl->free_count == ctl->capacity) ? 1 : 0;
+    ctl->n_new = n;
+    ctl->free_base = ctl->free_count - n;
+    ctl->free_count -= n;
+    ctl->g0 = ctl->next;
+    ctl->next += n;
+    ctl->iterations++;
+    work[0] = 0;
+    work[1] = 0;
+}
+
 // ------------------------------------------------------- wave builder ----
 
 struct Launch {
@@ -165,7 +226,7 @@ struct Wave {
     {
         const PathState& st = b->st;
         k_wave_begin<<<1, 128, 0, s>>>(st.counters, b->d_work, WORK_SLOTS);
-        k_pt_init<TECH, Ctx><<<(unsigned)((L.paths + 127) / 128), 128, 0, s>>>(ctx(b), st, 0);
+        k_pt_init<TECH, Ctx><<<(unsigned)((L.paths + 127) / 128), 128, 0, s>>>(ctx(b), st, 0, 0);
         int slot = 0;
         if (TECH != LMGPU_RENDER_PT) shadow(b, L, slot++, s);
         for (int k = 1; k <= K; k++, slot += 2) bounce(b, L, k, (k - 1) & 1, slot, s);
@@ -176,6 +237,49 @@ struct Wave {
     {
         k_pt_splat<FilmCtx><<<(unsigned)((L.paths + 127) / 128), 128, 0, s>>>(film_ctx(b), b->st, 0);
         k_wave_end<<<1, 1, 0, s>>>(b->d_wave, b->st.counters, b->d_stats);
+    }
+
+    static void warm(Launch& L)
+    {
+        L.trace_blocks = resident_blocks(k_trace_persistent<LAYOUT, STACK, false, PathRayIO<true>>);
+        L.shadow_blocks = resident_blocks(k_trace_persistent<LAYOUT, STACK, true, ShadowIO<FilmCtx>>);
+    }
+};
+
+template <int TECH, class F, int LAYOUT, int STACK>
+struct Stream {
+    using Ctx = StreamTable<float>;    // init / shade use no film
+    using FilmCtx = StreamTable<F>;
+
+    template <class C>
+    static C make(const LmgpuBatch* b)
+    {
+        return C{ b->d_table, b->d_begins, (int32_t)b->scenes.size(), b->d_ctl, b->st.sample, b->d_stats + 2 };
+    }
+
+    // One iteration with input queue q; traversal work counters work[2q], work[2q + 1].
+    static void iteration(const LmgpuBatch* b, const Launch& L, int q, cudaStream_t s)
+    {
+        const PathState& st = b->st;
+        unsigned long long* work = b->d_work + 2 * q;
+        k_stream_plan<<<1, 1, 0, s>>>(b->d_ctl, st.counters, q, b->d_stats, work);
+        k_pt_init<TECH, Ctx><<<(unsigned)((L.paths + 127) / 128), 128, 0, s>>>(make<Ctx>(b), st, 0, q);
+        PathRayIO<true> io{ st.queue[q], st.counters + q, st.ray_o, st.ray_d, st.hit, b->d_table, st.scene };
+        k_trace_persistent<LAYOUT, STACK, false, PathRayIO<true>><<<L.trace_blocks, 128, 0, s>>>(
+            L.proto, io, b->d_status, work);
+        k_pt_shade<TECH, Ctx><<<L.shade_blocks, 128, 0, s>>>(make<Ctx>(b), st, 0, q, 1 - q);
+        if (TECH != LMGPU_RENDER_PT) {
+            ShadowIO<FilmCtx> sio{ st.counters + 2, st.sh_o, st.sh_d, st.sh_c, st.L, make<FilmCtx>(b) };
+            k_trace_persistent<LAYOUT, STACK, true, ShadowIO<FilmCtx>><<<L.shadow_blocks, 128, 0, s>>>(
+                L.proto, sio, b->d_status, work + 1);
+        }
+        k_pt_retire<FilmCtx><<<L.shade_blocks, 128, 0, s>>>(make<FilmCtx>(b), st);
+    }
+
+    static void pair(const LmgpuBatch* b, const Launch& L, cudaStream_t s)
+    {
+        iteration(b, L, 0, s);
+        iteration(b, L, 1, s);
     }
 
     static void warm(Launch& L)
@@ -210,13 +314,17 @@ int ensure_batch_workspace(LmgpuBatch* b, int64_t paths)
     st.L = reinterpret_cast<float4*>(take(16 * P));
     st.prev_p = reinterpret_cast<float4*>(take(16 * P));
     st.prev_n = reinterpret_cast<float4*>(take(16 * P));
-    st.sh_o = reinterpret_cast<float4*>(take(16 * P));
-    st.sh_d = reinterpret_cast<float4*>(take(16 * P));
-    st.sh_c = reinterpret_cast<float4*>(take(16 * P));
+    st.sh_o = reinterpret_cast<float4*>(take(2 * 16 * P));
+    st.sh_d = reinterpret_cast<float4*>(take(2 * 16 * P));
+    st.sh_c = reinterpret_cast<float4*>(take(2 * 16 * P));
+    st.sample = reinterpret_cast<int64_t*>(take(8 * P));      // 8-byte arrays first: alignment
     st.raster = reinterpret_cast<float2*>(take(8 * P));
     st.queue[0] = reinterpret_cast<int32_t*>(take(4 * P));
     st.queue[1] = reinterpret_cast<int32_t*>(take(4 * P));
     st.scene = reinterpret_cast<int32_t*>(take(4 * P));
+    st.depth = reinterpret_cast<int32_t*>(take(4 * P));
+    st.free_slots = reinterpret_cast<int32_t*>(take(4 * P));
+    st.retire = reinterpret_cast<int32_t*>(take(4 * P));
     b->ws_capacity = paths;
     return LMGPU_OK;
 }
@@ -307,9 +415,66 @@ int upload_table(LmgpuBatch* b, const LmgpuRenderParams* params, void* const* fi
     return LMGPU_OK;
 }
 
+// Stream mode: `iterations` returns the iterations run (including at most
+// 2 * STREAM_CHECK_EVERY - 1 empty ones after the last path retired).
+template <int TECH, class F, int LAYOUT, int STACK>
+int run_stream(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_t& iterations)
+{
+    using S = Stream<TECH, F, LAYOUT, STACK>;
+    Launch L;
+    L.paths = P;
+    L.shade_blocks = std::max(1, b->cfg.shade_blocks_per_sm) * b->sms;
+    L.proto = b->scenes[0]->dev;
+    L.proto.layout = LAYOUT;
+    S::warm(L);
+    const unsigned setup_blocks = (unsigned)std::min<int64_t>((P + 255) / 256, 148 * 16);
+    k_stream_setup<<<setup_blocks, 256, 0, s>>>(b->d_ctl, pl.total, P, b->st.free_slots, b->st.counters, b->d_stats);
+    LMGPU_CUDA_TRY(cudaGetLastError());
+    if (b->cfg.use_graph) {
+        GraphKey key;
+        key.tech = TECH; key.fp64 = pl.fp64; key.layout = LAYOUT; key.stack = STACK; key.bounces = 0;
+        key.bounded = 0; key.shade_blocks = L.shade_blocks; key.paths = P; key.num_scenes = (int)b->scenes.size();
+        key.mode = LMGPU_BATCH_STREAM;
+        if (!b->exec || !(b->key == key)) {
+            if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; b->key = GraphKey{}; }
+            LMGPU_CUDA_TRY(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
+            S::pair(b, L, b->cap_stream);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(b->cap_stream, &g);
+            if (e != cudaSuccess) return cuda_fail(e, "graph capture of two stream iterations");
+            e = cudaGraphInstantiate(&b->exec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) { b->exec = nullptr; return cuda_fail(e, "cudaGraphInstantiate"); }
+            b->key = key;
+        }
+    }
+    // Every live path advances one bounce per iteration, so each slot's path
+    // ends within max_len + 1 iterations and every such period starts at
+    // least P samples: the bound below is never reached by a render that
+    // ends (Russian roulette makes a 1024-bounce path vanishingly unlikely).
+    const int64_t max_len = pl.bounded ? pl.bounces + 2 : 1024;
+    const int64_t bound = 2 * (((pl.total + P - 1) / P + 1) * (max_len + 1)) + 4 * STREAM_CHECK_EVERY;
+    int64_t launched = 0;
+    for (;;) {
+        for (int c = 0; c < STREAM_CHECK_EVERY; c++) {
+            if (b->cfg.use_graph) LMGPU_CUDA_TRY(cudaGraphLaunch(b->exec, s));
+            else S::pair(b, L, s);
+            launched += 2;
+        }
+        LMGPU_CUDA_TRY(cudaGetLastError());
+        LMGPU_CUDA_TRY(cudaMemcpyAsync(b->h_done, &b->d_ctl->iterations, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        LMGPU_CUDA_TRY(cudaStreamSynchronize(s));
+        if (b->h_done[1]) break;
+        if (launched > bound) return fail(LMGPU_ERR_TIMEOUT, "stream render did not end within its iteration bound");
+    }
+    iterations = b->h_done[0];
+    return LMGPU_OK;
+}
+
 template <int TECH, class F, int LAYOUT, int STACK>
 int run_waves(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_t& waves)
 {
+    if (b->cfg.mode == LMGPU_BATCH_STREAM) return run_stream<TECH, F, LAYOUT, STACK>(b, pl, P, s, waves);
     using W = Wave<TECH, F, LAYOUT, STACK>;
     Launch L;
     L.paths = P;
@@ -325,6 +490,7 @@ int run_waves(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_t&
         GraphKey key;
         key.tech = TECH; key.fp64 = pl.fp64; key.layout = LAYOUT; key.stack = STACK; key.bounces = pl.bounces;
         key.bounded = pl.bounded; key.shade_blocks = L.shade_blocks; key.paths = P; key.num_scenes = (int)b->scenes.size();
+        key.mode = LMGPU_BATCH_WAVES;
         if (!b->exec || !(b->key == key)) {
             if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; b->key = GraphKey{}; }
             LMGPU_CUDA_TRY(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
@@ -391,6 +557,7 @@ int check_config(const LmgpuBatchConfig& c)
         return fail(LMGPU_ERR_INVALID, "batch layout must be LMGPU_LAYOUT_BVH2 or LMGPU_LAYOUT_BVH4");
     if (c.wave_paths < 1024 || c.wave_paths > (1 << 26)) return fail(LMGPU_ERR_INVALID, "wave_paths must be in [1024, 2^26]");
     if (c.shade_blocks_per_sm < 1 || c.shade_blocks_per_sm > 64) return fail(LMGPU_ERR_INVALID, "shade_blocks_per_sm must be in [1, 64]");
+    if (c.mode != LMGPU_BATCH_WAVES && c.mode != LMGPU_BATCH_STREAM) return fail(LMGPU_ERR_INVALID, "unknown batch mode");
     return LMGPU_OK;
 }
 
@@ -476,6 +643,8 @@ int lmgpu_batch_create(LmgpuScene* const* scenes, int32_t num_scenes, LmgpuBatch
     dm(reinterpret_cast<void**>(&b->d_table), n * sizeof(BatchEntry));
     dm(reinterpret_cast<void**>(&b->d_begins), (n + 1) * sizeof(int64_t));
     dm(reinterpret_cast<void**>(&b->d_wave), sizeof(WaveCtl));
+    dm(reinterpret_cast<void**>(&b->d_ctl), sizeof(StreamCtl));
+    hm(reinterpret_cast<void**>(&b->h_done), 2 * sizeof(int64_t));
     dm(reinterpret_cast<void**>(&b->d_stats), NSTATS * sizeof(unsigned long long));
     dm(reinterpret_cast<void**>(&b->d_work), WORK_SLOTS * sizeof(unsigned long long));
     dm(reinterpret_cast<void**>(&b->d_status), sizeof(int32_t));
@@ -504,6 +673,8 @@ int lmgpu_batch_destroy(LmgpuBatch* b)
     cudaFree(b->d_table);
     cudaFree(b->d_begins);
     cudaFree(b->d_wave);
+    cudaFree(b->d_ctl);
+    cudaFreeHost(b->h_done);
     cudaFree(b->d_stats);
     cudaFree(b->d_work);
     cudaFree(b->d_status);
@@ -582,7 +753,14 @@ int lmgpu_batch_autotune(LmgpuBatch* b, const LmgpuRenderParams* params, double 
     best.use_graph = 1;
     double best_t = 1e30;
     rc = trial(best, best_t);
-    // Coordinate descent: layout, then wave size, then shading grid.
+    // Coordinate descent: mode, layout, then paths in flight, then shading grid.
+    for (int m : { LMGPU_BATCH_STREAM, LMGPU_BATCH_WAVES }) {
+        if (rc != LMGPU_OK || m == best.mode) continue;
+        LmgpuBatchConfig c = best;
+        c.mode = m;
+        double t;
+        if ((rc = trial(c, t)) == LMGPU_OK && t < best_t) { best = c; best_t = t; }
+    }
     const int layouts[] = { LMGPU_LAYOUT_BVH2, LMGPU_LAYOUT_BVH4 };
     const int waves[] = { 1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25 };
     const int grids[] = { 4, 8, 16 };

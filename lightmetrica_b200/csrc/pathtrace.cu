@@ -190,7 +190,7 @@ int render_waves(LmgpuScene* sc, const LmgpuRenderParams& p, F* film, cudaStream
         stats.paths += cnt;
         if (c.max_pv != -1 && c.max_pv <= 1) continue;   // no path vertex beyond the camera
         LMGPU_CUDA_TRY(cudaMemsetAsync(st.counters, 0, 16, stream));
-        k_pt_init<TECH, OneScene<F>><<<(unsigned)((cnt + 127) / 128), 128, 0, stream>>>(ctx, st, cnt);
+        k_pt_init<TECH, OneScene<F>><<<(unsigned)((cnt + 127) / 128), 128, 0, stream>>>(ctx, st, cnt, 0);
         LMGPU_CUDA_TRY(cudaGetLastError());
         if (TECH != LMGPU_RENDER_PT) {
             if ((rc = read_counts(ws, stream)) != LMGPU_OK) break;

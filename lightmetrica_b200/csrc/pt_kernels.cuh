@@ -16,7 +16,12 @@
 //   SceneTable<F>  a device table of scenes: a wave spans the samples of many
 //                  scenes, each path records its scene index, and the wave's
 //                  position comes from device memory, so one captured wave
-//                  replays unchanged (the multi-scene batch, batch.cu).
+//                  replays unchanged (the multi-scene batch, batch.cu);
+//   StreamTable<F> the same table with path regeneration: a fixed pool of
+//                  path slots, each path with its own sample index and
+//                  depth; finished paths retire (splat, free their slot) and
+//                  new camera paths take free slots every iteration, so the
+//                  queues stay full until the samples run out.
 // A sample's random numbers depend only on (seed, scene-local sample index,
 // dimension), so a scene renders the same paths alone or in a batch.
 #pragma once
@@ -50,7 +55,11 @@ struct PathState {
     float4* sh_d;      // direction, target (int bits: path index, or ~pixel)
     float4* sh_c;      // contribution, scene index (int bits)
     uint32_t* counters;   // [0], [1] ray queues; [2] shadow queue
-    int32_t* scene;    // per path scene index (SceneTable only)
+    int32_t* scene;    // per path scene index (SceneTable, StreamTable)
+    int64_t* sample;   // per path batch-global sample index (StreamTable)
+    int32_t* depth;    // per path index k of its next bounce (StreamTable)
+    int32_t* free_slots;   // free path slots (StreamTable)
+    int32_t* retire;   // paths finished this iteration (StreamTable; counters[3])
 };
 
 struct RenderConsts {
@@ -83,6 +92,14 @@ struct OneScene {
     __device__ __forceinline__ int path_scene(const PathState&, int64_t) const { return 0; }
     __device__ __forceinline__ int64_t sample_of(int, int64_t i) const { return rc.sample_base + i; }
     __device__ __forceinline__ F* film_of(int) const { return film; }
+    // New path number j of this launch: its slot i and scene-local sample.
+    __device__ __forceinline__ int begin_path(const PathState&, int64_t j, int64_t& i, int64_t& sample) const
+    {
+        i = j;
+        return locate(j, sample);
+    }
+    __device__ __forceinline__ int path_depth(const PathState&, int64_t, int k) const { return k; }
+    static constexpr bool STREAM = false;
 };
 
 // One scene of a batch as the kernels see it.
@@ -130,6 +147,66 @@ struct SceneTable {
         return table[sid].rc.sample_base + (wave->base + i - table[sid].begin);
     }
     __device__ __forceinline__ F* film_of(int sid) const { return static_cast<F*>(table[sid].film); }
+    __device__ __forceinline__ int begin_path(const PathState& st, int64_t j, int64_t& i, int64_t& sample) const
+    {
+        i = j;
+        const int sid = locate(j, sample);
+        st.scene[i] = sid;
+        return sid;
+    }
+    __device__ __forceinline__ int path_depth(const PathState&, int64_t, int k) const { return k; }
+    static constexpr bool STREAM = false;
+};
+
+// Plan of one regenerating iteration, written by a one-thread kernel.
+struct StreamCtl {
+    int64_t next;          // next batch-global sample to start
+    int64_t total;         // samples of the whole batch
+    int64_t free_count;    // free slots (free_slots[0, free_count))
+    int64_t n_new;         // paths started this iteration
+    int64_t free_base;     // they take free_slots[free_base, free_base + n_new)
+    int64_t g0;            // batch-global sample of the first of them
+    int64_t capacity;      // path slots
+    int64_t iterations;
+    int64_t done;          // all samples started and every slot free
+};
+
+template <class F>
+struct StreamTable {
+    static constexpr bool TABLE = true;
+    static constexpr bool STREAM = true;
+    const BatchEntry* table;
+    const int64_t* begins;
+    int32_t num_scenes;
+    const StreamCtl* ctl;
+    const int64_t* sample;            // PathState::sample
+    unsigned long long* max_depth;    // statistics: deepest bounce reached
+    __device__ __forceinline__ const DeviceScene& scene(int sid) const { return table[sid].s; }
+    __device__ __forceinline__ const RenderConsts& consts(int sid) const { return table[sid].rc; }
+    __device__ __forceinline__ int64_t wave_count(int64_t) const { return ctl->n_new; }
+    __device__ __forceinline__ int path_scene(const PathState& st, int64_t i) const { return st.scene[i]; }
+    __device__ __forceinline__ int64_t sample_of(int sid, int64_t i) const
+    {
+        return table[sid].rc.sample_base + (sample[i] - table[sid].begin);
+    }
+    __device__ __forceinline__ F* film_of(int sid) const { return static_cast<F*>(table[sid].film); }
+    __device__ __forceinline__ int begin_path(const PathState& st, int64_t j, int64_t& i, int64_t& local) const
+    {
+        i = st.free_slots[ctl->free_base + j];
+        const int64_t g = ctl->g0 + j;
+        int lo = 0, hi = num_scenes;    // begins[lo] <= g < begins[hi]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (begins[mid] <= g) lo = mid;
+            else hi = mid;
+        }
+        local = table[lo].rc.sample_base + (g - begins[lo]);
+        st.scene[i] = lo;
+        st.sample[i] = g;
+        st.depth[i] = 1;
+        return lo;
+    }
+    __device__ __forceinline__ int path_depth(const PathState& st, int64_t i, int) const { return st.depth[i]; }
 };
 
 // ------------------------------------------------------------- helpers ----
@@ -204,15 +281,15 @@ __device__ __forceinline__ bool camera_nee(const DeviceScene& s, uint64_t key, V
 
 // Wave initialisation: raster sample and camera ray; for pt.direct / pt.mis
 // the whole camera vertex (light sample, Russian roulette). `count` is the
-// wave's path count for OneScene (SceneTable reads it from the device).
+// wave's path count for OneScene (the tables read it from the device); new
+// rays join ray queue q.
 template <int TECH, class Ctx>
-__global__ void __launch_bounds__(128) k_pt_init(const Ctx ctx, const PathState st, int64_t count)
+__global__ void __launch_bounds__(128) k_pt_init(const Ctx ctx, const PathState st, int64_t count, int q)
 {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= ctx.wave_count(count)) return;
-    int64_t sample;
-    const int sid = ctx.locate(i, sample);
-    if (Ctx::TABLE) st.scene[i] = sid;
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ctx.wave_count(count)) return;
+    int64_t sample, i;
+    const int sid = ctx.begin_path(st, j, i, sample);
     const DeviceScene& s = ctx.scene(sid);
     const RenderConsts& rc = ctx.consts(sid);
     const uint64_t key = sample_key(rc.seed, (uint64_t)sample);
@@ -249,11 +326,15 @@ __global__ void __launch_bounds__(128) k_pt_init(const Ctx ctx, const PathState 
         st.prev_n[i] = make_float4(0, 0, 1, __uint_as_float(PREV_DEGENERATED));
     }
     st.thr[i] = f4(thr, 0.0f);
-    const uint32_t slot = queue_append(&st.counters[0], alive);
+    const uint32_t slot = queue_append(&st.counters[q], alive);
     if (alive) {
         st.ray_o[i] = f4(cp, TECH == LMGPU_RENDER_PT ? 0.0f : EPS_F);
         st.ray_d[i] = f4(dir, 0.0f);
-        st.queue[0][slot] = (int32_t)i;
+        st.queue[q][slot] = (int32_t)i;
+    }
+    if (Ctx::STREAM) {                           // a path that ends at the camera retires at once
+        const uint32_t r = queue_append(&st.counters[3], !alive);
+        if (!alive) st.retire[r] = (int32_t)i;
     }
 }
 
@@ -350,7 +431,7 @@ struct ShadowIO {
 // and BSDF sampling; pt samples the BSDF first and applies Russian roulette
 // with numPathVertices = k (pathtrace.cpp:223-260).
 template <int TECH, class Ctx>
-__global__ void __launch_bounds__(128) k_pt_shade(const Ctx ctx, const PathState st, int k, int qin, int qout)
+__global__ void __launch_bounds__(128) k_pt_shade(const Ctx ctx, const PathState st, int kw, int qin, int qout)
 {
     const int64_t count = (int64_t)st.counters[qin];
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -361,6 +442,7 @@ __global__ void __launch_bounds__(128) k_pt_shade(const Ctx ctx, const PathState
         const bool valid = j < count;
         const int32_t i = valid ? st.queue[qin][j] : 0;
         const int sid = valid ? ctx.path_scene(st, i) : 0;
+        const int k = valid ? ctx.path_depth(st, i, kw) : kw;   // this bounce's index
         bool alive = false, shadow = false;
         V3 thr = v3(0, 0, 0), L = v3(0, 0, 0);
         Geom g;
@@ -476,7 +558,32 @@ __global__ void __launch_bounds__(128) k_pt_shade(const Ctx ctx, const PathState
                 st.prev_n[i] = f4(g.sn, __uint_as_float(bs.specular ? PREV_SPECULAR : 0u));
             }
             st.queue[qout][slot] = i;
+            if (Ctx::STREAM) st.depth[i] = k + 1;
         }
+        if constexpr (Ctx::STREAM) {
+            const bool done = valid && !alive;
+            const uint32_t r = queue_append(&st.counters[3], done);
+            if (done) st.retire[r] = i;
+            const unsigned m = __reduce_max_sync(__activemask(), valid ? (unsigned)k : 0u);
+            if ((threadIdx.x & 31u) == (unsigned)(__ffs(__activemask()) - 1)) atomicMax(ctx.max_depth, (unsigned long long)m);
+        }
+    }
+}
+
+// Retirement of the paths that finished this iteration (after the shadow
+// pass, whose contributions they have received): splat their radiance and
+// return their slots to the free list after the slots still free.
+template <class Ctx>
+__global__ void __launch_bounds__(128) k_pt_retire(const Ctx ctx, const PathState st)
+{
+    const int64_t n = (int64_t)st.counters[3];
+    const int64_t base = ctx.ctl->free_count;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t i = st.retire[j];
+        const int sid = ctx.path_scene(st, i);
+        const float2 r = st.raster[i];
+        film_add(ctx.film_of(sid), film_pixel(ctx.scene(sid).cam, r.x, r.y), f3(st.L[i]));
+        st.free_slots[base + j] = i;
     }
 }
 

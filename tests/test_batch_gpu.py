@@ -88,10 +88,13 @@ def test_batch_matches_one_scene_renders(cuda, technique):
 
 @pytest.mark.parametrize("config", [
     dict(layout="qbvh"),
-    dict(wave_paths=4096),                       # many waves, every wave spans scenes
+    dict(wave_paths=4096),                       # stream: slots recycled many times, across scenes
     dict(wave_paths=1 << 20, shade_blocks_per_sm=2),
     dict(use_graph=False),
     dict(layout="qbvh", wave_paths=10000, use_graph=False),
+    dict(mode="waves"),
+    dict(mode="waves", wave_paths=4096),         # many waves, every wave spans scenes
+    dict(mode="waves", layout="qbvh", wave_paths=10000, use_graph=False),
 ])
 def test_batch_configurations_agree(cuda, config):
     items = small_set()
@@ -104,16 +107,36 @@ def test_batch_configurations_agree(cuda, config):
     batch.close()
 
 
-def test_batch_unbounded_depth_tail(cuda):
-    """max_path_vertices = -1 (Russian roulette only): the graph covers the
-    first bounces and direct launches finish the deep tail."""
+@pytest.mark.parametrize("mode", ["waves", "stream"])
+def test_batch_unbounded_depth_tail(cuda, mode):
+    """max_path_vertices = -1 (Russian roulette only): in wave mode the graph
+    covers the first bounces and direct launches finish the deep tail; in
+    stream mode every path simply lives until it ends."""
     items = [(scenes.cornell_box(32, 32, variant="mixed"), renderer("pt.mis", 1, -1, 5), 32 * 32 * 32),
              (scenes.cornell_box(24, 24), renderer("pt.mis", 1, -1, 6), 24 * 24 * 16)]
     built = [build(p) for p, _, _ in items]
     want = plain_films(built, items)
     batch = SceneBatch(built)
-    batch.configure(wave_paths=8192)
+    batch.configure(wave_paths=8192, mode=mode)
     assert_same(batch_films(batch, items), want)
+    batch.close()
+
+
+def test_stream_mode_statistics(cuda):
+    """Stream mode counts the same rays as wave mode (same paths) and reports
+    its iterations."""
+    items = small_set()
+    built = [build(p) for p, _, _ in items]
+    batch = SceneBatch(built)
+    stats = {}
+    for mode in ("waves", "stream"):
+        batch.configure(mode=mode, wave_paths=8192)
+        batch_films(batch, items)
+        stats[mode] = dict(batch.last_stats)
+    assert stats["stream"]["rays_traced"] == stats["waves"]["rays_traced"]
+    assert stats["stream"]["shadow_rays"] == stats["waves"]["shadow_rays"]
+    assert stats["stream"]["max_bounces_run"] == stats["waves"]["max_bounces_run"]
+    assert stats["stream"]["waves"] > 8     # iterations
     batch.close()
 
 
@@ -141,7 +164,7 @@ def test_batch_autotune_keeps_results(cuda):
     want = plain_films(built, items)
     batch = SceneBatch(built)
     cfg = batch.autotune([r for _, r, _ in items], [n for _, _, n in items], sample_fraction=0.25)
-    assert cfg["layout"] in ("bvh", "qbvh") and cfg["trial_ms"] > 0
+    assert cfg["layout"] in ("bvh", "qbvh") and cfg["trial_ms"] > 0 and cfg["mode"] in ("waves", "stream")
     assert cfg["wave_paths"] in (1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25)
     assert_same(batch_films(batch, items), want)
     batch.close()
