@@ -296,14 +296,15 @@ typedef struct LmgpuBatchConfig {
     int32_t shade_blocks_per_sm;  /* grid of the shading kernel (blocks of 128 threads per SM) */
     int32_t use_graph;            /* 1: replay a captured CUDA graph (a wave, or two stream
                                      iterations); 0: direct launches */
-    int32_t mode;                 /* LMGPU_BATCH_STREAM (default) or LMGPU_BATCH_WAVES */
+    int32_t mode;                 /* LMGPU_BATCH_WAVES (default) or LMGPU_BATCH_STREAM */
 } LmgpuBatchConfig;
 
 /* The scenes (built with a BVH layout, on the current device) must outlive
  * the batch; a scene may appear more than once. Default configuration:
  * BVH2, 2^24 paths in flight (about 3 GB of path state), 16 shading blocks
- * per SM, graphs on, path regeneration; a device short of memory gets
- * fewer paths in flight. */
+ * per SM, graphs on, fixed waves (stream mode keeps every slot busy, but its
+ * recycled slots scatter path state in memory: slower on the benchmark
+ * scenes); a device short of memory gets fewer paths in flight. */
 int lmgpu_batch_create(LmgpuScene* const* scenes, int32_t num_scenes, LmgpuBatch** out);
 int lmgpu_batch_destroy(LmgpuBatch* batch);
 int lmgpu_batch_get_config(const LmgpuBatch* batch, LmgpuBatchConfig* config);

@@ -13,7 +13,7 @@
 // unbounded (max_path_vertices = -1) finish their tail bounces with direct
 // launches after the graph.
 //
-// Stream mode (the default) regenerates paths instead: the path slots form
+// Stream mode regenerates paths instead: the path slots form
 // one pool, every iteration retires the paths that finished (splat, free the
 // slot) and starts new camera paths in the free slots, so the ray queues
 // stay full until the samples run out and only the batch's last paths run
@@ -66,7 +66,7 @@ struct LmgpuBatch {
     int device = 0;
     int sms = 148;
     std::vector<LmgpuScene*> scenes;
-    LmgpuBatchConfig cfg{ LMGPU_LAYOUT_BVH2, 1 << 24, 16, 1, LMGPU_BATCH_STREAM };
+    LmgpuBatchConfig cfg{ LMGPU_LAYOUT_BVH2, 1 << 24, 16, 1, LMGPU_BATCH_WAVES };
 
     BatchEntry* d_table = nullptr;
     int64_t* d_begins = nullptr;
@@ -754,7 +754,7 @@ int lmgpu_batch_autotune(LmgpuBatch* b, const LmgpuRenderParams* params, double 
     double best_t = 1e30;
     rc = trial(best, best_t);
     // Coordinate descent: mode, layout, then paths in flight, then shading grid.
-    for (int m : { LMGPU_BATCH_STREAM, LMGPU_BATCH_WAVES }) {
+    for (int m : { LMGPU_BATCH_WAVES, LMGPU_BATCH_STREAM }) {
         if (rc != LMGPU_OK || m == best.mode) continue;
         LmgpuBatchConfig c = best;
         c.mode = m;
