@@ -430,8 +430,12 @@ struct ShadowIO {
 // then for pt.direct / pt.mis next-event estimation at it, Russian roulette
 // and BSDF sampling; pt samples the BSDF first and applies Russian roulette
 // with numPathVertices = k (pathtrace.cpp:223-260).
+#ifndef LMGPU_PT_SHADE_MIN_BLOCKS
+#define LMGPU_PT_SHADE_MIN_BLOCKS 8      // 64 registers: more resident warps for the latency-bound gathers
+#endif
 template <int TECH, class Ctx>
-__global__ void __launch_bounds__(128) k_pt_shade(const Ctx ctx, const PathState st, int kw, int qin, int qout)
+__global__ void __launch_bounds__(128, LMGPU_PT_SHADE_MIN_BLOCKS) k_pt_shade(const Ctx ctx, const PathState st, int kw,
+                                                                            int qin, int qout)
 {
     const int64_t count = (int64_t)st.counters[qin];
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
