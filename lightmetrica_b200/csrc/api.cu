@@ -457,7 +457,7 @@ int ensure_host_pipeline(LmgpuScene* sc)
     HostPipeline& hp = sc->pipe;
     if (hp.ready) return LMGPU_OK;
     hp.chunk = int64_t(1) << 20;   // 1M rays: 32 MB in, 16 MB out per stage
-    for (int k = 0; k < 2; k++) {
+    for (int k = 0; k < HostPipeline::SLOTS; k++) {
         LMGPU_CUDA_TRY(cudaStreamCreateWithFlags(&hp.stream[k], cudaStreamNonBlocking));
         void* p = nullptr;
         LMGPU_CUDA_TRY(cudaMalloc(&p, (size_t)hp.chunk * 12 * sizeof(float)));
@@ -502,7 +502,7 @@ int lmgpu_scene_destroy(LmgpuScene* scene)
 {
     if (!scene) return LMGPU_OK;
     if (scene->pipe.ready)
-        for (int k = 0; k < 2; k++) cudaStreamDestroy(scene->pipe.stream[k]);
+        for (int k = 0; k < HostPipeline::SLOTS; k++) cudaStreamDestroy(scene->pipe.stream[k]);
     for (void* p : scene->allocations) cudaFree(p);
     delete scene;
     return LMGPU_OK;
@@ -534,16 +534,16 @@ int lmgpu_intersect_host(LmgpuScene* scene, const float* rays_aos, int64_t n, in
 {
     if (!scene || (n > 0 && !rays_aos) || n < 0) return fail(LMGPU_ERR_INVALID, "null argument or negative count");
     if (n == 0) return LMGPU_OK;
-    // Chunked two-stream pipeline: the H2D copy of chunk c+1 and the D2H copy
-    // of chunk c-1 overlap the traversal of chunk c. Staging buffers are
-    // cached in the scene and grown on demand.
+    // Chunked pipeline over HostPipeline::SLOTS streams: uploads, traversals
+    // and downloads of neighbouring chunks overlap (full-duplex PCIe).
+    // Staging buffers are cached in the scene.
     int rc = ensure_host_pipeline(scene);
     if (rc != LMGPU_OK) return rc;
     HostPipeline& hp = scene->pipe;
     const int64_t chunk = hp.chunk;
     const int64_t nchunks = (n + chunk - 1) / chunk;
     for (int64_t c = 0; c < nchunks && rc == LMGPU_OK; c++) {
-        const int k = static_cast<int>(c & 1);
+        const int k = static_cast<int>(c % HostPipeline::SLOTS);
         cudaStream_t st = hp.stream[k];
         const int64_t b = c * chunk, m = std::min(chunk, n - b);
         float* dr = hp.rays[k];
@@ -563,7 +563,7 @@ int lmgpu_intersect_host(LmgpuScene* scene, const float* rays_aos, int64_t n, in
             if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemcpyAsync(hits)");
         }
     }
-    for (int k = 0; k < 2; k++) {
+    for (int k = 0; k < HostPipeline::SLOTS; k++) {
         cudaError_t e = cudaStreamSynchronize(hp.stream[k]);
         if (e != cudaSuccess && rc == LMGPU_OK) rc = cuda_fail(e, "cudaStreamSynchronize");
     }

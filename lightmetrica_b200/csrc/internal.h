@@ -7,14 +7,17 @@
 #include "../../include/lmgpu.h"
 #include "scene.cuh"
 
-// Staging for the host-buffer entry points: two streams, each with a device
-// chunk of AoS rays and SoA hits.
+// Staging for the host-buffer entry points: SLOTS streams, each with a
+// device chunk of AoS rays and SoA hits. With four slots the upload of chunk
+// c + 2 does not queue behind the download of chunk c, so both copy
+// directions stay busy at once.
 struct HostPipeline {
+    static constexpr int SLOTS = 4;
     bool ready = false;
     int64_t chunk = 0;
-    cudaStream_t stream[2] = { nullptr, nullptr };
-    float* rays[2] = { nullptr, nullptr };
-    float* hits[2] = { nullptr, nullptr };
+    cudaStream_t stream[SLOTS] = {};
+    float* rays[SLOTS] = {};
+    float* hits[SLOTS] = {};
 };
 
 struct LmgpuScene {
