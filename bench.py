@@ -59,6 +59,10 @@ def parse():
     ap.add_argument("--render-spp", type=int, default=64, help="spp of the 1080p section (profiling runs use less)")
     ap.add_argument("--render-frames", type=int, default=3, help="timed frames of the 1080p section")
     ap.add_argument("--no-render-parity", action="store_true", help="skip the 1080p section's relMSE image")
+    ap.add_argument("--batch-fraction", type=float, default=1.0,
+                    help="scale every batch scene's sample count (profiling runs use less)")
+    ap.add_argument("--batch-only", action="store_true",
+                    help="batch section: only the batch, default configuration (profiling runs)")
     ap.add_argument("--sections", default="render,adjoint,batch",
                     help="extra single-GPU sections in the same line: render (1080p path tracer), "
                          "adjoint (forward/backward cost), batch (64-scene batch vs plain); '' for none")
@@ -563,7 +567,7 @@ def batch_section(args, dev):
         r.configure({"rr_depth": 5, "max_path_vertices": d["max_path_vertices"], "sampler": {"rng_seed": i + 1}})
         rs.append(r)
         W = d["prims"].camera.film.width
-        ns.append(W * W * d["spp"])
+        ns.append(max(1, int(W * W * d["spp"] * args.batch_fraction)))
         films.append(torch.zeros(W * W * 3, dtype=torch.float32, device=dev))
     setup_s = time.perf_counter() - t0
     stream = torch.cuda.current_stream(dev)
@@ -591,6 +595,16 @@ def batch_section(args, dev):
         b.record(stream)
         torch.cuda.synchronize()
         return a.elapsed_time(b), out
+
+    if args.batch_only:
+        batch = SceneBatch(built)
+        batch.render_device(rs, ns, films)
+        batch_ms, _ = timed(lambda: batch.render_device(rs, ns, films, stats=False))
+        batch.close()
+        for sc in built:
+            sc.close()
+        return {"workload": "64-scene batch only (profiling run)", "samples": total, "batched_ms": round(batch_ms, 2),
+                "config": "default"}
 
     # Plain wavefront, one scene at a time.
     zero()
