@@ -93,16 +93,37 @@ __device__ __forceinline__ bool slab_intrinsic(const TraversalRay& r,
 #ifndef LMGPU_TRACE_FAST_SLAB
 #define LMGPU_TRACE_FAST_SLAB 1
 #endif
+#ifndef LMGPU_TRACE_F32X2
+#define LMGPU_TRACE_F32X2 1
+#endif
+// (lo - o) * inv and (hi - o) * inv: with LMGPU_TRACE_F32X2 as one packed
+// sub.rn.f32x2 and one mul.rn.f32x2 (sm_100), each lane rounded to nearest
+// on its own, i.e. the same two results as the scalar __fsub_rn/__fmul_rn.
+__device__ __forceinline__ void plane_pair(float lo, float hi, float o, float inv, float& a, float& b)
+{
+#if LMGPU_TRACE_F32X2
+    asm("{\n\t.reg .b64 p, q;\n\t"
+        "mov.b64 p, {%2, %3};\n\t"
+        "mov.b64 q, {%4, %4};\n\t"
+        "sub.rn.f32x2 p, p, q;\n\t"
+        "mov.b64 q, {%5, %5};\n\t"
+        "mul.rn.f32x2 p, p, q;\n\t"
+        "mov.b64 {%0, %1}, p;\n\t}"
+        : "=f"(a), "=f"(b) : "f"(lo), "f"(hi), "f"(o), "f"(inv));
+#else
+    a = __fmul_rn(__fsub_rn(lo, o), inv);
+    b = __fmul_rn(__fsub_rn(hi, o), inv);
+#endif
+}
+
 __device__ __forceinline__ bool slab_finite(const TraversalRay& r,
                                             float lox, float hix, float loy, float hiy,
                                             float loz, float hiz, float& t_enter)
 {
-    const float ax = __fmul_rn(__fsub_rn(lox, r.o[0]), r.inv_min[0]);
-    const float bx = __fmul_rn(__fsub_rn(hix, r.o[0]), r.inv_min[0]);
-    const float ay = __fmul_rn(__fsub_rn(loy, r.o[1]), r.inv_min[1]);
-    const float by = __fmul_rn(__fsub_rn(hiy, r.o[1]), r.inv_min[1]);
-    const float az = __fmul_rn(__fsub_rn(loz, r.o[2]), r.inv_min[2]);
-    const float bz = __fmul_rn(__fsub_rn(hiz, r.o[2]), r.inv_min[2]);
+    float ax, bx, ay, by, az, bz;
+    plane_pair(lox, hix, r.o[0], r.inv_min[0], ax, bx);
+    plane_pair(loy, hiy, r.o[1], r.inv_min[1], ay, by);
+    plane_pair(loz, hiz, r.o[2], r.inv_min[2], az, bz);
     const float tn = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fminf(az, bz));
     const float tf = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
     t_enter = tn;
