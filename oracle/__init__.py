@@ -30,10 +30,13 @@ _LL = ctypes.c_longlong
 
 def build(reference_root: str = "/root/reference") -> None:
     """Compile the C restatement and, when the reference tree is present, the
-    reference harness (oracle/_ref). Building the checker is not using it."""
+    reference harness (oracle/_ref) and the product's lightmetrica plugin
+    built against the reference headers (oracle/_ref/plugin.gpu.so).
+    Building the checker is not using it."""
     subprocess.run(["bash", os.path.join(HERE, "build_oracle.sh")], check=True)
     if os.path.isdir(os.path.join(reference_root, "src", "liblightmetrica")):
         subprocess.run(["bash", os.path.join(HERE, "build_ref.sh"), reference_root], check=True)
+        subprocess.run(["bash", os.path.join(HERE, "build_plugin.sh"), reference_root], check=True)
 
 
 def _ptr(a):
@@ -174,6 +177,29 @@ class RefScene:
         return out
 
 
+PLUGIN_SO = os.path.join(HERE, "_ref", "plugin.gpu.so")
+_plugins_loaded = set()
+
+
+def plugin_available() -> bool:
+    return os.path.exists(PLUGIN_SO) and ref_available("f")
+
+
+def load_plugin(path: str = PLUGIN_SO) -> None:
+    """Loads a lightmetrica plugin into the float reference build the way the
+    reference does (dlopen, then its exported LM_Plugin_CreateInstance): its
+    components become available to RefScene and ref_render by name."""
+    if path in _plugins_loaded:
+        return
+    L = ref("f")
+    L.lmref_load_plugin.restype = ctypes.c_int
+    L.lmref_load_plugin.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_char_p)]
+    err = ctypes.c_char_p()
+    if L.lmref_load_plugin(path.encode(), ctypes.byref(err)) != 0:
+        raise RuntimeError(f"plugin {path} failed to load: {err.value.decode() if err.value else ''}")
+    _plugins_loaded.add(path)
+
+
 def stub_random_mesh():
     """The reference test fixture StubTriangleMesh_Random (1000 triangles)."""
     p = np.zeros(9000, np.float32)
@@ -195,7 +221,7 @@ class _RefRenderDesc(ctypes.Structure):
                 ("width", ctypes.c_int), ("height", ctypes.c_int), ("renderer", ctypes.c_char_p),
                 ("rr_depth", ctypes.c_int), ("max_path_vertices", ctypes.c_int), ("seed", ctypes.c_int),
                 ("num_samples", ctypes.c_longlong), ("num_threads", ctypes.c_int),
-                ("samples_per_block", ctypes.c_longlong)]
+                ("samples_per_block", ctypes.c_longlong), ("scene_type", ctypes.c_char_p)]
 
 
 def flatten_primitives(prims):
@@ -242,9 +268,11 @@ def flatten_primitives(prims):
 
 
 def ref_render(prims, renderer="pt", num_samples=None, spp=16, rr_depth=1, max_path_vertices=-1, seed=1,
-               threads=None, precision="d", samples_per_block=100):
+               threads=None, precision="d", samples_per_block=100, scene_type="bvh"):
     """Renders `prims` with the reference's own renderer + `mt` scheduler
-    (oracle/_ref). Returns (film (H, W, 3) float32, render seconds)."""
+    (oracle/_ref) over the accelerator `scene_type` (the reference's "bvh",
+    or a loaded plugin's scene such as "plugin.gpu"). Returns (film (H, W, 3)
+    float32, render seconds)."""
     L = ref(precision)
     if not hasattr(L, "lmref_render"):
         raise RuntimeError("reference harness built without the renderer")
@@ -294,6 +322,7 @@ def ref_render(prims, renderer="pt", num_samples=None, spp=16, rr_depth=1, max_p
     d.num_samples = int(num_samples if num_samples is not None else spp * W * H)
     d.num_threads = int(threads or os.cpu_count() or 1)
     d.samples_per_block = samples_per_block
+    d.scene_type = scene_type.encode()
     film = np.zeros((H, W, 3), np.float32)
     bt = ctypes.c_double()
     secs = L.lmref_render(ctypes.byref(d), film.ctypes.data, ctypes.byref(bt))

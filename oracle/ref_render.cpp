@@ -67,6 +67,7 @@ struct RefRenderDesc {
     long long num_samples;
     int num_threads;
     long long samples_per_block;
+    const char* scene_type;             // accelerator ("bvh" when null), e.g. a plugin's "plugin.gpu"
 };
 }
 
@@ -288,7 +289,8 @@ double lmref_render(const RefRenderDesc* d, float* film_out, double* build_secon
     }
 
     // Scene
-    std::unique_ptr<Scene> scene(ComponentFactory::Create<Scene>("bvh"));
+    std::unique_ptr<Scene> scene(ComponentFactory::Create<Scene>(d->scene_type ? d->scene_type : "bvh"));
+    if (!scene) return -7;
     scene->Load(P);
     auto tb0 = std::chrono::high_resolution_clock::now();
     if (!scene->Configure(ConfigNode()) || !scene->Build() || !scene->PostConfigure()) return -6;

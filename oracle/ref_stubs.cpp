@@ -10,6 +10,8 @@
 //     by a small in-memory tree (HarnessNode) instead of pugixml.
 // Everything here is written for this harness; only the declarations it
 // implements come from the reference headers.
+#include <dlfcn.h>
+#include <vector>
 #include <lightmetrica/logger.h>
 #include <lightmetrica/component.h>
 #include <lightmetrica/confignode.h>
@@ -57,10 +59,27 @@ bool ComponentFactory::Register(const std::string& interfaceType, const std::str
 	return true;
 }
 
+// Plugins loaded by lmref_load_plugin: their exported entry points
+// (plugin.common.cpp:97-110), asked after the internal registry, in load
+// order, like the reference's factory (component.cpp:152-166).
+struct LoadedPlugin {
+	void* handle;
+	Component* (*create)(const char* implType, const char* interfaceType);
+	bool (*check)(const char* implType, const char* interfaceType);
+};
+static std::vector<LoadedPlugin>& Plugins()
+{
+	static std::vector<LoadedPlugin> p;
+	return p;
+}
+
 Component* ComponentFactory::Create(const std::string& interfaceType, const std::string& implType)
 {
 	auto it = Registry().find(Key(interfaceType, implType));
-	return it == Registry().end() ? nullptr : it->second();
+	if (it != Registry().end()) return it->second();
+	for (auto& p : Plugins())
+		if (p.check(implType.c_str(), interfaceType.c_str())) return p.create(implType.c_str(), interfaceType.c_str());
+	return nullptr;
 }
 
 void ComponentFactory::LoadPlugins(const std::string&) {}
@@ -201,6 +220,33 @@ bool PluginManager::Register(const std::string& interfaceType, const std::string
 	return ComponentFactory::Register(interfaceType, implType, func);
 }
 LM_NAMESPACE_END
+
+// Loads a plugin the way the reference does (dlopen with RTLD_LAZY |
+// RTLD_LOCAL, dynamiclibrary.cpp:78) and adds it to the factory's search.
+// Returns 0, or -1 with the loader's message in *error.
+extern "C" int lmref_load_plugin(const char* path, const char** error)
+{
+	static std::string msg;
+	void* h = dlopen(path, RTLD_LAZY | RTLD_LOCAL);
+	if (!h) { msg = dlerror(); if (error) *error = msg.c_str(); return -1; }
+	lightmetrica::LoadedPlugin p;
+	p.handle = h;
+	p.create = reinterpret_cast<lightmetrica::Component* (*)(const char*, const char*)>(dlsym(h, "LM_Plugin_CreateInstance"));
+	p.check = reinterpret_cast<bool (*)(const char*, const char*)>(dlsym(h, "LM_Plugin_CheckRegistered"));
+	if (!p.create || !p.check) { msg = "missing plugin entry points"; if (error) *error = msg.c_str(); return -1; }
+	lightmetrica::Plugins().push_back(p);
+	return 0;
+}
+
+// 1 if the factory (internal registry, then loaded plugins) can create
+// implType of interfaceType; the instance is created and destroyed.
+extern "C" int lmref_component_available(const char* interfaceType, const char* implType)
+{
+	lightmetrica::Component* c = lightmetrica::ComponentFactory::Create(interfaceType, implType);
+	if (!c) return 0;
+	delete c;
+	return 1;
+}
 
 // Diagnostics: the registered component keys ("interface::impl"), newline-separated.
 extern "C" const char* lmref_registered_components()
