@@ -23,10 +23,10 @@ pytestmark = [pytest.mark.gpu,
 def test_plugin_scene_equals_reference_bvh_bit_for_bit(cuda):
     oracle.load_plugin()
     pos, faces = random_soup(4096, seed=7, sigma=0.1)
-    rays = random_rays(20000, seed=8)
+    rays = random_rays(4000, seed=8)
     ref = oracle.RefScene(pos, faces, "bvh").intersect(rays, geom=True, threads=1)
     got = oracle.RefScene(pos, faces, "plugin.gpu").intersect(rays, geom=True, threads=4)
-    assert (ref["tri_id"] >= 0).sum() > 2000
+    assert (ref["tri_id"] >= 0).sum() > 400
     np.testing.assert_array_equal(got["tri_id"], ref["tri_id"])
     np.testing.assert_array_equal(got["t"], ref["t"])
     for k in ("p", "gn", "sn", "ss", "st", "uv"):
