@@ -305,6 +305,10 @@ double lmref_render(const RefRenderDesc* d, float* film_out, double* build_secon
         n->Add("num_threads", std::to_string(d->num_threads));
         n->Add("samples_per_block", std::to_string(d->samples_per_block > 0 ? d->samples_per_block : 100));
         if (!sched->Configure(ConfigNode(n, nullptr), assets)) return -7;
+        // The reference leaves terminationMode uninitialised (sched.mt.cpp:58)
+        // and its application always sets it (main.cpp:500); so does this
+        // harness, or the render loop's exit depends on heap contents.
+        sched->SetTerminationMode(TerminationMode::Samples, 0);
     }
     std::unique_ptr<Renderer> renderer(ComponentFactory::Create<Renderer>(d->renderer));
     if (!renderer) return -8;
