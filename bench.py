@@ -606,12 +606,21 @@ def batch_section(args, dev):
         return {"workload": "64-scene batch only (profiling run)", "samples": total, "batched_ms": round(batch_ms, 2),
                 "config": "default"}
 
-    # Plain wavefront, one scene at a time.
+    # Batch configuration from the autotuner (untimed, like a build step).
+    batch = SceneBatch(built)
+    t0 = time.perf_counter()
+    tuned = batch.autotune(rs, ns, sample_fraction=1.0 / 16)
+    tune_s = time.perf_counter() - t0
+
+    # One untimed pass of each renderer: warm-up, films for the comparison,
+    # the batch's ray statistics.
     zero()
-    plain_pass()                                          # warm-up
-    zero()
-    plain_ms, plain_rays = timed(plain_pass)
+    plain_pass()
     plain = [f.clone() for f in films]
+    zero()
+    batch.render_device(rs, ns, films)
+    st = batch.last_stats
+    batched = [f.clone() for f in films]
 
     # Plain megakernel, one launch per scene (scene's own albedo and emission).
     drs = [DifferentiableRender(sc, r, n) for sc, r, n in zip(built, rs, ns)]
@@ -621,21 +630,22 @@ def batch_section(args, dev):
     def mega_pass():
         return [dr.forward(a, e) for dr, (a, e) in zip(drs, params)]
     mega_pass()
-    mega_ms, _ = timed(mega_pass)
 
-    # Batch: autotune (untimed, like a build step), warm-up, timed render.
-    batch = SceneBatch(built)
-    t0 = time.perf_counter()
-    tuned = batch.autotune(rs, ns, sample_fraction=1.0 / 16)
-    tune_s = time.perf_counter() - t0
-    zero()
-    batch.render_device(rs, ns, films)
-    zero()
-    batch_ms, _ = timed(lambda: batch.render_device(rs, ns, films, stats=False))
-    batch.render_device(rs, ns, [torch.zeros_like(f) for f in films])     # stats of one render
-    st = batch.last_stats
+    # Timed: the three renderers in turn, `rounds` times, best time of each
+    # (clocks and temperature drift by several percent over a run this long;
+    # taking turns gives every renderer the same conditions).
+    rounds = 3
+    plain_ms = mega_ms = batch_ms = float("inf")
+    plain_rays = 0
+    for _ in range(rounds):
+        ms, plain_rays = timed(plain_pass)
+        plain_ms = min(plain_ms, ms)
+        ms, _ = timed(mega_pass)
+        mega_ms = min(mega_ms, ms)
+        ms, _ = timed(lambda: batch.render_device(rs, ns, films, stats=False))
+        batch_ms = min(batch_ms, ms)
     rel = []
-    for a, b in zip(films, plain):
+    for a, b in zip(batched, plain):
         a64, b64 = a.double(), b.double()
         rel.append(float(((a64 - b64) ** 2 / (b64 ** 2 + 1e-2)).mean()))
     batch.close()
@@ -652,7 +662,7 @@ def batch_section(args, dev):
             "batched_Msamples_per_s": round(total / (batch_ms / 1e3) / 1e6, 1),
             "plain_wavefront_Mrays_per_s": round(plain_rays / (plain_ms / 1e3) / 1e6, 1),
             "waves": st["waves"], "autotuned": tuned, "autotune_seconds": round(tune_s, 2),
-            "setup_seconds": round(setup_s, 2),
+            "setup_seconds": round(setup_s, 2), "timing": f"best of {rounds} rounds, the three renderers in turn",
             "relMSE_batched_vs_plain_max": max(rel),
             "equal_relMSE": "same samples and paths in both; films differ only by float-atomic summation order"}
 

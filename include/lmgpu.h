@@ -286,17 +286,24 @@ typedef struct LmgpuBatch LmgpuBatch;
 
 enum {
     LMGPU_BATCH_WAVES = 0,   /* fixed waves: each wave's paths run to the end before the next wave */
-    LMGPU_BATCH_STREAM = 1   /* path regeneration: finished paths' slots take new paths every
+    LMGPU_BATCH_STREAM = 1,  /* path regeneration: finished paths' slots take new paths every
                                 iteration, so the queues stay full until the samples run out */
+    LMGPU_BATCH_OVERLAP = 2  /* fixed waves in two path pools: a wave's tail (its bounces from
+                                overlap_bounce on, where few paths are left) runs beside the
+                                next wave's first bounces; twice the path-state memory.
+                                Renders with unbounded depth run as LMGPU_BATCH_WAVES. */
 };
 
 typedef struct LmgpuBatchConfig {
     int32_t layout;               /* LMGPU_LAYOUT_BVH2 or LMGPU_LAYOUT_BVH4 for every scene */
-    int32_t wave_paths;           /* paths in flight: the capacity of the ray and shadow queues */
+    int32_t wave_paths;           /* paths in flight: the capacity of the ray and shadow queues
+                                     (per pool) */
     int32_t shade_blocks_per_sm;  /* grid of the shading kernel (blocks of 128 threads per SM) */
     int32_t use_graph;            /* 1: replay a captured CUDA graph (a wave, or two stream
                                      iterations); 0: direct launches */
-    int32_t mode;                 /* LMGPU_BATCH_WAVES (default) or LMGPU_BATCH_STREAM */
+    int32_t mode;                 /* LMGPU_BATCH_WAVES (default), _STREAM or _OVERLAP */
+    int32_t overlap_bounce;       /* LMGPU_BATCH_OVERLAP: first bounce of a wave's tail, in
+                                     [1, 64]; 0 = automatic (3) */
 } LmgpuBatchConfig;
 
 /* The scenes (built with a BVH layout, on the current device) must outlive
@@ -321,7 +328,7 @@ int lmgpu_batch_render_device(LmgpuBatch* batch, const LmgpuRenderParams* params
 
 /* Autotuner: renders the batch with each scene's sample count scaled by
  * `sample_fraction` (0 < f <= 1) under candidate configurations (mode, BVH
- * layout, paths in flight, shading grid), coordinate by coordinate, keeps the
+ * layout, paths in flight, shading grid, overlap bounce), coordinate by coordinate, keeps the
  * fastest, stores it as the batch's configuration and returns it with its
  * device time in ms. Films are scratch memory of the tuner; synchronises. */
 int lmgpu_batch_autotune(LmgpuBatch* batch, const LmgpuRenderParams* params, double sample_fraction,

@@ -9,9 +9,11 @@ sched.mt.cpp:93-266).
 Each scene keeps its own camera, film, renderer parameters (technique shared
 by the batch) and sample count, and renders exactly the samples it would
 render alone through RenderProcessScheduler.render: same random numbers,
-same paths. All scenes' paths share one pool of path slots ("stream" mode:
-finished paths' slots take new paths every iteration) or fixed waves
-("waves"), and the kernel sequence is replayed from a captured CUDA graph.
+same paths. All scenes' paths run in fixed waves ("waves"), in fixed waves
+over two pools of path state whose tails overlap the next wave's first
+bounces ("overlap"), or in one pool of path slots that take new paths as
+old ones finish ("stream"); the kernel sequence is replayed from a captured
+CUDA graph.
 """
 from __future__ import annotations
 
@@ -24,6 +26,7 @@ from . import native as N
 from .render import Renderer
 
 LAYOUTS = {"bvh": N.LAYOUT_BVH2, "qbvh": N.LAYOUT_BVH4}
+MODES = {"waves": N.BATCH_WAVES, "stream": N.BATCH_STREAM, "overlap": N.BATCH_OVERLAP}
 
 
 class SceneBatch:
@@ -44,11 +47,11 @@ class SceneBatch:
         N.check(N.lib().lmgpu_batch_get_config(self.handle, ctypes.byref(c)))
         return {"layout": {v: k for k, v in LAYOUTS.items()}[c.layout], "wave_paths": c.wave_paths,
                 "shade_blocks_per_sm": c.shade_blocks_per_sm, "use_graph": bool(c.use_graph),
-                "mode": {N.BATCH_WAVES: "waves", N.BATCH_STREAM: "stream"}[c.mode]}
+                "mode": {v: k for k, v in MODES.items()}[c.mode], "overlap_bounce": c.overlap_bounce}
 
     def configure(self, layout: str | None = None, wave_paths: int | None = None,
                   shade_blocks_per_sm: int | None = None, use_graph: bool | None = None,
-                  mode: str | None = None) -> None:
+                  mode: str | None = None, overlap_bounce: int | None = None) -> None:
         c = N.BatchConfig()
         N.check(N.lib().lmgpu_batch_get_config(self.handle, ctypes.byref(c)))
         if layout is not None:
@@ -62,9 +65,11 @@ class SceneBatch:
         if use_graph is not None:
             c.use_graph = 1 if use_graph else 0
         if mode is not None:
-            if mode not in ("waves", "stream"):
-                raise ValueError("mode must be 'waves' or 'stream'")
-            c.mode = N.BATCH_WAVES if mode == "waves" else N.BATCH_STREAM
+            if mode not in MODES:
+                raise ValueError("mode must be 'waves', 'stream' or 'overlap'")
+            c.mode = MODES[mode]
+        if overlap_bounce is not None:
+            c.overlap_bounce = int(overlap_bounce)
         N.check(N.lib().lmgpu_batch_set_config(self.handle, ctypes.byref(c)))
 
     # ------------------------------------------------------------ render --
@@ -118,7 +123,7 @@ class SceneBatch:
         return out
 
     def autotune(self, renderers, num_samples, sample_fraction: float = 0.125, stream=None) -> dict:
-        """Chooses layout, wave size and shading grid by timing scaled-down
+        """Chooses mode, layout, wave size, shading grid and overlap bounce by timing scaled-down
         renders of this batch; the choice becomes the batch's configuration."""
         import torch
         params = self._params(renderers, num_samples, False)

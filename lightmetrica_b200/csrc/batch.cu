@@ -13,6 +13,10 @@
 // unbounded (max_path_vertices = -1) finish their tail bounces with direct
 // launches after the graph.
 //
+// Overlap mode keeps two pools of path state and runs each wave's
+// latency-bound tail bounces beside the next wave's first bounces (two
+// branches of one captured graph).
+//
 // Stream mode regenerates paths instead: the path slots form
 // one pool, every iteration retires the paths that finished (splat, free the
 // slot) and starts new camera paths in the free slots, so the ray queues
@@ -36,6 +40,8 @@ using namespace lmgpu;
 namespace {
 
 constexpr int WORK_SLOTS = 160;            // traversal launches per wave: 2 per bounce + 1
+constexpr int POOLS = 2;                   // path pools (overlap mode uses both)
+constexpr int DEFAULT_OVERLAP_BOUNCE = 3;
 constexpr int GRAPH_BOUNCES_UNBOUNDED = 24;
 constexpr int MAX_BOUNDED_BOUNCES = 64;
 // path state + scene index + sample index, depth, free list, retire queue;
@@ -50,13 +56,14 @@ constexpr int NSTATS = 4;
 
 struct GraphKey {
     int tech = -1, fp64 = -1, layout = -1, stack = -1, bounces = -1, bounded = -1, shade_blocks = -1, mode = -1;
+    int split = -1;
     int64_t paths = -1;
     int num_scenes = -1;
     bool operator==(const GraphKey& o) const
     {
         return tech == o.tech && fp64 == o.fp64 && layout == o.layout && stack == o.stack && bounces == o.bounces &&
                bounded == o.bounded && shade_blocks == o.shade_blocks && paths == o.paths && num_scenes == o.num_scenes &&
-               mode == o.mode;
+               mode == o.mode && split == o.split;
     }
 };
 
@@ -66,15 +73,15 @@ struct LmgpuBatch {
     int device = 0;
     int sms = 148;
     std::vector<LmgpuScene*> scenes;
-    LmgpuBatchConfig cfg{ LMGPU_LAYOUT_BVH2, 1 << 24, 16, 1, LMGPU_BATCH_WAVES };
+    LmgpuBatchConfig cfg{ LMGPU_LAYOUT_BVH2, 1 << 24, 16, 1, LMGPU_BATCH_WAVES, 0 };
 
     BatchEntry* d_table = nullptr;
     int64_t* d_begins = nullptr;
-    WaveCtl* d_wave = nullptr;
+    WaveCtl* d_wave = nullptr;              // one per path pool
     StreamCtl* d_ctl = nullptr;
     int64_t* h_done = nullptr;              // pinned: StreamCtl::done and ::iterations
     unsigned long long* d_stats = nullptr;
-    unsigned long long* d_work = nullptr;
+    unsigned long long* d_work = nullptr;   // WORK_SLOTS per path pool
     int32_t* d_status = nullptr;
     BatchEntry* h_table = nullptr;          // pinned staging
     int64_t* h_begins = nullptr;
@@ -83,11 +90,19 @@ struct LmgpuBatch {
     cudaEvent_t staged = nullptr;           // the staging buffers' last copy has run
 
     void* ws_mem = nullptr;
-    int64_t ws_capacity = 0;
-    PathState st{};
+    int64_t ws_capacity = 0;                // paths per pool
+    int ws_pools = 0;
+    PathState st[POOLS]{};
 
     cudaStream_t cap_stream = nullptr;
-    cudaGraphExec_t exec = nullptr;
+    // Overlap period branches: heads at the highest stream priority, tails
+    // at the lowest (captured kernel nodes keep their stream's priority).
+    cudaStream_t cap_hi = nullptr, cap_lo = nullptr;    // for capture
+    cudaStream_t hi = nullptr, lo = nullptr;            // for direct launches
+    cudaEvent_t ev[5] = {};                 // overlap period: fork, tail 0, head 1, head branch end, tail branch end
+    cudaGraphExec_t exec = nullptr;         // a wave, two stream iterations, or an overlap period
+    cudaGraphExec_t exec_head = nullptr;    // overlap: pool 0's first head
+    cudaGraphExec_t exec_tail = nullptr;    // overlap: pool 0's last tail
     GraphKey key;
 };
 
@@ -95,12 +110,18 @@ namespace {
 
 // ------------------------------------------------------ small kernels ----
 
-__global__ void k_batch_setup(WaveCtl* wave, int64_t total, int64_t step, unsigned long long* stats)
+// Pool l starts at wave l; each pool then advances by `pools` waves.
+__global__ void k_batch_setup(WaveCtl* wave, int pools, int64_t total, int64_t step, unsigned long long* stats)
 {
-    wave->base = 0;
-    wave->count = step < total ? step : total;
-    wave->total = total;
-    wave->step = step;
+    for (int l = 0; l < pools; l++) {
+        const int64_t base = l * step;
+        const int64_t left = total - base;
+        wave[l].base = base;
+        wave[l].count = left <= 0 ? 0 : (left < step ? left : step);
+        wave[l].total = total;
+        wave[l].step = step;
+        wave[l].stride = pools * step;
+    }
     for (int i = 0; i < NSTATS; i++) stats[i] = 0;
 }
 
@@ -113,23 +134,25 @@ __global__ void k_wave_begin(uint32_t* counters, unsigned long long* work, int s
 }
 
 // Before bounce k: tally the rays about to be traced and the shadow rays of
-// the previous pass, then clear the output queue and the shadow queue.
+// the previous pass, then clear the output queue and the shadow queue. The
+// totals are shared by the path pools (atomics: pools run concurrently).
 __global__ void k_bounce_prep(uint32_t* counters, int qin, int k, unsigned long long* stats)
 {
     const uint32_t n = counters[qin];
-    stats[0] += n;
-    stats[1] += counters[2];
-    if (n > 0 && (unsigned long long)k > stats[2]) stats[2] = (unsigned long long)k;
+    atomicAdd(stats + 0, (unsigned long long)n);
+    atomicAdd(stats + 1, (unsigned long long)counters[2]);
+    if (n > 0) atomicMax(stats + 2, (unsigned long long)k);
     counters[1 - qin] = 0;
     counters[2] = 0;
 }
 
-// End of a wave (after the splat): last shadow tally, advance to the next wave.
+// End of a wave (after the splat): last shadow tally, advance the pool to
+// its next wave.
 __global__ void k_wave_end(WaveCtl* wave, uint32_t* counters, unsigned long long* stats)
 {
-    stats[1] += counters[2];
+    atomicAdd(stats + 1, (unsigned long long)counters[2]);
     counters[2] = 0;
-    const int64_t base = wave->base + wave->step;
+    const int64_t base = wave->base + wave->stride;
     wave->base = base;
     const int64_t left = wave->total - base;
     wave->count = left <= 0 ? 0 : (left < wave->step ? left : wave->step);
@@ -191,52 +214,71 @@ struct Launch {
     DeviceScene proto;         // template scene for the traversal kernel (layout only)
 };
 
+// One wave of path pool l: head = begin, init, camera shadow pass, bounces
+// 1 .. T-1; tail = bounces T .. K, splat, advance. The traversal launches of
+// bounce k use work slots slot_of(k) and slot_of(k) + 1 of the pool.
 template <int TECH, class F, int LAYOUT, int STACK>
 struct Wave {
     using Ctx = SceneTable<float>;     // init / shade use no film
     using FilmCtx = SceneTable<F>;
 
-    static Ctx ctx(const LmgpuBatch* b) { return Ctx{ b->d_table, b->d_begins, (int32_t)b->scenes.size(), b->d_wave }; }
-    static FilmCtx film_ctx(const LmgpuBatch* b)
+    static Ctx ctx(const LmgpuBatch* b, int l)
     {
-        return FilmCtx{ b->d_table, b->d_begins, (int32_t)b->scenes.size(), b->d_wave };
+        return Ctx{ b->d_table, b->d_begins, (int32_t)b->scenes.size(), b->d_wave + l };
     }
-
-    static void shadow(const LmgpuBatch* b, const Launch& L, int slot, cudaStream_t s)
+    static FilmCtx film_ctx(const LmgpuBatch* b, int l)
     {
-        const PathState& st = b->st;
-        ShadowIO<FilmCtx> io{ st.counters + 2, st.sh_o, st.sh_d, st.sh_c, st.L, film_ctx(b) };
+        return FilmCtx{ b->d_table, b->d_begins, (int32_t)b->scenes.size(), b->d_wave + l };
+    }
+    static unsigned long long* work(const LmgpuBatch* b, int l) { return b->d_work + (size_t)l * WORK_SLOTS; }
+    static int slot_of(int k) { return (TECH != LMGPU_RENDER_PT ? 1 : 0) + 2 * (k - 1); }
+
+    static void shadow(const LmgpuBatch* b, const Launch& L, int l, int slot, cudaStream_t s)
+    {
+        const PathState& st = b->st[l];
+        ShadowIO<FilmCtx> io{ st.counters + 2, st.sh_o, st.sh_d, st.sh_c, st.L, film_ctx(b, l) };
         k_trace_persistent<LAYOUT, STACK, true, ShadowIO<FilmCtx>><<<L.shadow_blocks, 128, 0, s>>>(
-            L.proto, io, b->d_status, b->d_work + slot);
+            L.proto, io, b->d_status, work(b, l) + slot);
     }
 
-    static void bounce(const LmgpuBatch* b, const Launch& L, int k, int qin, int slot, cudaStream_t s)
+    static void bounce(const LmgpuBatch* b, const Launch& L, int l, int k, int slot, cudaStream_t s)
     {
-        const PathState& st = b->st;
+        const PathState& st = b->st[l];
+        const int qin = (k - 1) & 1;
         k_bounce_prep<<<1, 1, 0, s>>>(st.counters, qin, k, b->d_stats);
         PathRayIO<true> io{ st.queue[qin], st.counters + qin, st.ray_o, st.ray_d, st.hit, b->d_table, st.scene };
         k_trace_persistent<LAYOUT, STACK, false, PathRayIO<true>><<<L.trace_blocks, 128, 0, s>>>(
-            L.proto, io, b->d_status, b->d_work + slot);
-        k_pt_shade<TECH, Ctx><<<L.shade_blocks, 128, 0, s>>>(ctx(b), st, k, qin, 1 - qin);
-        if (TECH != LMGPU_RENDER_PT) shadow(b, L, slot + 1, s);
+            L.proto, io, b->d_status, work(b, l) + slot);
+        k_pt_shade<TECH, Ctx><<<L.shade_blocks, 128, 0, s>>>(ctx(b, l), st, k, qin, 1 - qin);
+        if (TECH != LMGPU_RENDER_PT) shadow(b, L, l, slot + 1, s);
     }
 
-    // init + bounces 1..K (+ splat and wave advance when `finish`).
+    static void head(const LmgpuBatch* b, const Launch& L, int l, int T, cudaStream_t s)
+    {
+        const PathState& st = b->st[l];
+        k_wave_begin<<<1, 128, 0, s>>>(st.counters, work(b, l), WORK_SLOTS);
+        k_pt_init<TECH, Ctx><<<(unsigned)((L.paths + 127) / 128), 128, 0, s>>>(ctx(b, l), st, 0, 0);
+        if (TECH != LMGPU_RENDER_PT) shadow(b, L, l, 0, s);
+        for (int k = 1; k < T; k++) bounce(b, L, l, k, slot_of(k), s);
+    }
+
+    static void tail(const LmgpuBatch* b, const Launch& L, int l, int T, int K, cudaStream_t s)
+    {
+        for (int k = T; k <= K; k++) bounce(b, L, l, k, slot_of(k), s);
+        tail_end(b, L, l, s);
+    }
+
+    // Pool 0: init + bounces 1..K (+ splat and wave advance when `finish`).
     static void body(const LmgpuBatch* b, const Launch& L, int K, bool finish, cudaStream_t s)
     {
-        const PathState& st = b->st;
-        k_wave_begin<<<1, 128, 0, s>>>(st.counters, b->d_work, WORK_SLOTS);
-        k_pt_init<TECH, Ctx><<<(unsigned)((L.paths + 127) / 128), 128, 0, s>>>(ctx(b), st, 0, 0);
-        int slot = 0;
-        if (TECH != LMGPU_RENDER_PT) shadow(b, L, slot++, s);
-        for (int k = 1; k <= K; k++, slot += 2) bounce(b, L, k, (k - 1) & 1, slot, s);
-        if (finish) tail_end(b, L, s);
+        head(b, L, 0, K + 1, s);
+        if (finish) tail_end(b, L, 0, s);
     }
 
-    static void tail_end(const LmgpuBatch* b, const Launch& L, cudaStream_t s)
+    static void tail_end(const LmgpuBatch* b, const Launch& L, int l, cudaStream_t s)
     {
-        k_pt_splat<FilmCtx><<<(unsigned)((L.paths + 127) / 128), 128, 0, s>>>(film_ctx(b), b->st, 0);
-        k_wave_end<<<1, 1, 0, s>>>(b->d_wave, b->st.counters, b->d_stats);
+        k_pt_splat<FilmCtx><<<(unsigned)((L.paths + 127) / 128), 128, 0, s>>>(film_ctx(b, l), b->st[l], 0);
+        k_wave_end<<<1, 1, 0, s>>>(b->d_wave + l, b->st[l].counters, b->d_stats);
     }
 
     static void warm(Launch& L)
@@ -254,13 +296,13 @@ struct Stream {
     template <class C>
     static C make(const LmgpuBatch* b)
     {
-        return C{ b->d_table, b->d_begins, (int32_t)b->scenes.size(), b->d_ctl, b->st.sample, b->d_stats + 2 };
+        return C{ b->d_table, b->d_begins, (int32_t)b->scenes.size(), b->d_ctl, b->st[0].sample, b->d_stats + 2 };
     }
 
     // One iteration with input queue q; traversal work counters work[2q], work[2q + 1].
     static void iteration(const LmgpuBatch* b, const Launch& L, int q, cudaStream_t s)
     {
-        const PathState& st = b->st;
+        const PathState& st = b->st[0];
         unsigned long long* work = b->d_work + 2 * q;
         k_stream_plan<<<1, 1, 0, s>>>(b->d_ctl, st.counters, q, b->d_stats, work);
         k_pt_init<TECH, Ctx><<<(unsigned)((L.paths + 127) / 128), 128, 0, s>>>(make<Ctx>(b), st, 0, q);
@@ -291,41 +333,71 @@ struct Stream {
 
 // ------------------------------------------------------------ driver ------
 
-int ensure_batch_workspace(LmgpuBatch* b, int64_t paths)
+void drop_graphs(LmgpuBatch* b)
 {
-    if (b->ws_capacity >= paths && b->ws_mem) return LMGPU_OK;
-    if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; b->key = GraphKey{}; }
-    if (b->ws_mem) { cudaFree(b->ws_mem); b->ws_mem = nullptr; b->ws_capacity = 0; }
+    for (cudaGraphExec_t* g : { &b->exec, &b->exec_head, &b->exec_tail })
+        if (*g) { cudaGraphExecDestroy(*g); *g = nullptr; }
+    b->key = GraphKey{};
+}
+
+// Path state of `paths` paths in each of `pools` pools (at least the pools
+// and capacity already held), one allocation; every pool starts on a
+// 256-byte boundary.
+int ensure_batch_workspace(LmgpuBatch* b, int64_t paths, int pools)
+{
+    if (b->ws_mem && b->ws_capacity >= paths && b->ws_pools >= pools) return LMGPU_OK;
+    pools = std::max(pools, b->ws_pools);
+    drop_graphs(b);
+    if (b->ws_mem) { cudaFree(b->ws_mem); b->ws_mem = nullptr; b->ws_capacity = 0; b->ws_pools = 0; }
     const size_t P = (size_t)paths;
-    cudaError_t e = cudaMalloc(&b->ws_mem, P * BYTES_PER_PATH + 256);
+    const size_t pool_bytes = (256 + P * BYTES_PER_PATH + 255) / 256 * 256;
+    cudaError_t e = cudaMalloc(&b->ws_mem, pool_bytes * pools);
     if (e != cudaSuccess) {
         b->ws_mem = nullptr;
         return e == cudaErrorMemoryAllocation ? fail(LMGPU_ERR_OOM, "batch workspace allocation failed")
                                               : cuda_fail(e, "cudaMalloc(batch workspace)");
     }
-    char* p = static_cast<char*>(b->ws_mem);
-    auto take = [&](size_t n) { char* r = p; p += n; return r; };
-    PathState& st = b->st;
-    st.counters = reinterpret_cast<uint32_t*>(take(256));
-    st.ray_o = reinterpret_cast<float4*>(take(16 * P));
-    st.ray_d = reinterpret_cast<float4*>(take(16 * P));
-    st.hit = reinterpret_cast<float4*>(take(16 * P));
-    st.thr = reinterpret_cast<float4*>(take(16 * P));
-    st.L = reinterpret_cast<float4*>(take(16 * P));
-    st.prev_p = reinterpret_cast<float4*>(take(16 * P));
-    st.prev_n = reinterpret_cast<float4*>(take(16 * P));
-    st.sh_o = reinterpret_cast<float4*>(take(2 * 16 * P));
-    st.sh_d = reinterpret_cast<float4*>(take(2 * 16 * P));
-    st.sh_c = reinterpret_cast<float4*>(take(2 * 16 * P));
-    st.sample = reinterpret_cast<int64_t*>(take(8 * P));      // 8-byte arrays first: alignment
-    st.raster = reinterpret_cast<float2*>(take(8 * P));
-    st.queue[0] = reinterpret_cast<int32_t*>(take(4 * P));
-    st.queue[1] = reinterpret_cast<int32_t*>(take(4 * P));
-    st.scene = reinterpret_cast<int32_t*>(take(4 * P));
-    st.depth = reinterpret_cast<int32_t*>(take(4 * P));
-    st.free_slots = reinterpret_cast<int32_t*>(take(4 * P));
-    st.retire = reinterpret_cast<int32_t*>(take(4 * P));
+    for (int l = 0; l < pools; l++) {
+        char* p = static_cast<char*>(b->ws_mem) + pool_bytes * l;
+        auto take = [&](size_t n) { char* r = p; p += n; return r; };
+        PathState& st = b->st[l];
+        st.counters = reinterpret_cast<uint32_t*>(take(256));
+        st.ray_o = reinterpret_cast<float4*>(take(16 * P));
+        st.ray_d = reinterpret_cast<float4*>(take(16 * P));
+        st.hit = reinterpret_cast<float4*>(take(16 * P));
+        st.thr = reinterpret_cast<float4*>(take(16 * P));
+        st.L = reinterpret_cast<float4*>(take(16 * P));
+        st.prev_p = reinterpret_cast<float4*>(take(16 * P));
+        st.prev_n = reinterpret_cast<float4*>(take(16 * P));
+        st.sh_o = reinterpret_cast<float4*>(take(2 * 16 * P));
+        st.sh_d = reinterpret_cast<float4*>(take(2 * 16 * P));
+        st.sh_c = reinterpret_cast<float4*>(take(2 * 16 * P));
+        st.sample = reinterpret_cast<int64_t*>(take(8 * P));      // 8-byte arrays first: alignment
+        st.raster = reinterpret_cast<float2*>(take(8 * P));
+        st.queue[0] = reinterpret_cast<int32_t*>(take(4 * P));
+        st.queue[1] = reinterpret_cast<int32_t*>(take(4 * P));
+        st.scene = reinterpret_cast<int32_t*>(take(4 * P));
+        st.depth = reinterpret_cast<int32_t*>(take(4 * P));
+        st.free_slots = reinterpret_cast<int32_t*>(take(4 * P));
+        st.retire = reinterpret_cast<int32_t*>(take(4 * P));
+    }
     b->ws_capacity = paths;
+    b->ws_pools = pools;
+    return LMGPU_OK;
+}
+
+// Captures what `fn` launches on the capture stream into *out.
+template <class Fn>
+int capture(LmgpuBatch* b, Fn fn, cudaGraphExec_t* out, const char* what, unsigned long long flags = 0)
+{
+    LMGPU_CUDA_TRY(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
+    fn(b->cap_stream);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(b->cap_stream, &g);
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    e = cudaGraphInstantiate(out, g, flags);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { *out = nullptr; return cuda_fail(e, "cudaGraphInstantiate"); }
     return LMGPU_OK;
 }
 
@@ -428,7 +500,7 @@ int run_stream(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_t
     L.proto.layout = LAYOUT;
     S::warm(L);
     const unsigned setup_blocks = (unsigned)std::min<int64_t>((P + 255) / 256, 148 * 16);
-    k_stream_setup<<<setup_blocks, 256, 0, s>>>(b->d_ctl, pl.total, P, b->st.free_slots, b->st.counters, b->d_stats);
+    k_stream_setup<<<setup_blocks, 256, 0, s>>>(b->d_ctl, pl.total, P, b->st[0].free_slots, b->st[0].counters, b->d_stats);
     LMGPU_CUDA_TRY(cudaGetLastError());
     if (b->cfg.use_graph) {
         GraphKey key;
@@ -436,15 +508,10 @@ int run_stream(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_t
         key.bounded = 0; key.shade_blocks = L.shade_blocks; key.paths = P; key.num_scenes = (int)b->scenes.size();
         key.mode = LMGPU_BATCH_STREAM;
         if (!b->exec || !(b->key == key)) {
-            if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; b->key = GraphKey{}; }
-            LMGPU_CUDA_TRY(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
-            S::pair(b, L, b->cap_stream);
-            cudaGraph_t g = nullptr;
-            cudaError_t e = cudaStreamEndCapture(b->cap_stream, &g);
-            if (e != cudaSuccess) return cuda_fail(e, "graph capture of two stream iterations");
-            e = cudaGraphInstantiate(&b->exec, g, 0);
-            cudaGraphDestroy(g);
-            if (e != cudaSuccess) { b->exec = nullptr; return cuda_fail(e, "cudaGraphInstantiate"); }
+            drop_graphs(b);
+            const int rc = capture(b, [&](cudaStream_t c) { S::pair(b, L, c); }, &b->exec,
+                                   "graph capture of two stream iterations");
+            if (rc != LMGPU_OK) return rc;
             b->key = key;
         }
     }
@@ -471,10 +538,92 @@ int run_stream(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_t
     return LMGPU_OK;
 }
 
+// Overlap mode: pool 0 renders waves 0, 2, 4, ..., pool 1 waves 1, 3, 5, ...;
+// a wave splits at bounce T into head (init, bounces 1 .. T-1) and tail
+// (bounces T .. K, splat). One period runs two branches,
+//     heads (high priority):  head(2j + 1) -> head(2j + 2)   (after tail(2j): same pool)
+//     tails (low priority):   tail(2j)     -> tail(2j + 1)   (after head(2j + 1))
+// so each wave's latency-bound tail shares the GPU with the other pool's
+// full-width head, and the block scheduler serves the head's kernels
+// first. Pool 0's first head comes before the periods and its last tail
+// after them; floor(W / 2) periods cover W waves (a wave past the last
+// sample has no paths and costs only its launches). Depth must be
+// bounded: the tail is a fixed sequence of bounces.
+template <int TECH, class F, int LAYOUT, int STACK>
+int run_overlap(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_t& waves)
+{
+    using W = Wave<TECH, F, LAYOUT, STACK>;
+    Launch L;
+    L.paths = P;
+    L.shade_blocks = std::max(1, b->cfg.shade_blocks_per_sm) * b->sms;
+    L.proto = b->scenes[0]->dev;
+    L.proto.layout = LAYOUT;
+    W::warm(L);
+    const int K = pl.bounces;
+    const int T = std::min(b->cfg.overlap_bounce > 0 ? b->cfg.overlap_bounce : DEFAULT_OVERLAP_BOUNCE, K + 1);
+    waves = (pl.total + P - 1) / P;
+    const int64_t periods = waves / 2;
+    k_batch_setup<<<1, 1, 0, s>>>(b->d_wave, POOLS, pl.total, P, b->d_stats);
+    LMGPU_CUDA_TRY(cudaGetLastError());
+
+    auto head0 = [&](cudaStream_t a) { W::head(b, L, 0, T, a); };
+    auto tail0 = [&](cudaStream_t a) { W::tail(b, L, 0, T, K, a); };
+    // Event calls inside a capture fail only with the capture, which the
+    // capture's end reports; for direct launches they are checked after.
+    auto period = [&](cudaStream_t a, cudaStream_t hi, cudaStream_t lo) {
+        cudaEvent_t* ev = b->ev;
+        cudaEventRecord(ev[0], a);
+        cudaStreamWaitEvent(hi, ev[0], 0);
+        cudaStreamWaitEvent(lo, ev[0], 0);
+        W::tail(b, L, 0, T, K, lo);
+        cudaEventRecord(ev[1], lo);
+        W::head(b, L, 1, T, hi);
+        cudaEventRecord(ev[2], hi);
+        cudaStreamWaitEvent(hi, ev[1], 0);
+        W::head(b, L, 0, T, hi);
+        cudaEventRecord(ev[3], hi);
+        cudaStreamWaitEvent(lo, ev[2], 0);
+        W::tail(b, L, 1, T, K, lo);
+        cudaEventRecord(ev[4], lo);
+        cudaStreamWaitEvent(a, ev[3], 0);
+        cudaStreamWaitEvent(a, ev[4], 0);
+    };
+    if (b->cfg.use_graph) {
+        GraphKey key;
+        key.tech = TECH; key.fp64 = pl.fp64; key.layout = LAYOUT; key.stack = STACK; key.bounces = K;
+        key.bounded = 1; key.shade_blocks = L.shade_blocks; key.paths = P; key.num_scenes = (int)b->scenes.size();
+        key.mode = LMGPU_BATCH_OVERLAP; key.split = T;
+        if (!b->exec || !b->exec_head || !b->exec_tail || !(b->key == key)) {
+            drop_graphs(b);
+            int rc = capture(b, head0, &b->exec_head, "graph capture of a wave head");
+            if (rc == LMGPU_OK)
+                rc = capture(b, [&](cudaStream_t a) { period(a, b->cap_hi, b->cap_lo); }, &b->exec,
+                             "graph capture of an overlap period", cudaGraphInstantiateFlagUseNodePriority);
+            if (rc == LMGPU_OK) rc = capture(b, tail0, &b->exec_tail, "graph capture of a wave tail");
+            if (rc != LMGPU_OK) { drop_graphs(b); return rc; }
+            b->key = key;
+        }
+        LMGPU_CUDA_TRY(cudaGraphLaunch(b->exec_head, s));
+        for (int64_t j = 0; j < periods; j++) LMGPU_CUDA_TRY(cudaGraphLaunch(b->exec, s));
+        LMGPU_CUDA_TRY(cudaGraphLaunch(b->exec_tail, s));
+        return LMGPU_OK;
+    }
+    head0(s);
+    LMGPU_CUDA_TRY(cudaGetLastError());
+    for (int64_t j = 0; j < periods; j++) {
+        period(s, b->hi, b->lo);
+        LMGPU_CUDA_TRY(cudaGetLastError());
+    }
+    tail0(s);
+    LMGPU_CUDA_TRY(cudaGetLastError());
+    return LMGPU_OK;
+}
+
 template <int TECH, class F, int LAYOUT, int STACK>
 int run_waves(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_t& waves)
 {
     if (b->cfg.mode == LMGPU_BATCH_STREAM) return run_stream<TECH, F, LAYOUT, STACK>(b, pl, P, s, waves);
+    if (b->cfg.mode == LMGPU_BATCH_OVERLAP && pl.bounded) return run_overlap<TECH, F, LAYOUT, STACK>(b, pl, P, s, waves);
     using W = Wave<TECH, F, LAYOUT, STACK>;
     Launch L;
     L.paths = P;
@@ -483,7 +632,7 @@ int run_waves(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_t&
     L.proto.layout = LAYOUT;
     W::warm(L);
     waves = (pl.total + P - 1) / P;
-    k_batch_setup<<<1, 1, 0, s>>>(b->d_wave, pl.total, P, b->d_stats);
+    k_batch_setup<<<1, 1, 0, s>>>(b->d_wave, 1, pl.total, P, b->d_stats);
     LMGPU_CUDA_TRY(cudaGetLastError());
 
     if (b->cfg.use_graph) {
@@ -492,15 +641,10 @@ int run_waves(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_t&
         key.bounded = pl.bounded; key.shade_blocks = L.shade_blocks; key.paths = P; key.num_scenes = (int)b->scenes.size();
         key.mode = LMGPU_BATCH_WAVES;
         if (!b->exec || !(b->key == key)) {
-            if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; b->key = GraphKey{}; }
-            LMGPU_CUDA_TRY(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
-            W::body(b, L, pl.bounces, pl.bounded, b->cap_stream);
-            cudaGraph_t g = nullptr;
-            cudaError_t e = cudaStreamEndCapture(b->cap_stream, &g);
-            if (e != cudaSuccess) return cuda_fail(e, "graph capture of a batch wave");
-            e = cudaGraphInstantiate(&b->exec, g, 0);
-            cudaGraphDestroy(g);
-            if (e != cudaSuccess) { b->exec = nullptr; return cuda_fail(e, "cudaGraphInstantiate"); }
+            drop_graphs(b);
+            const int rc = capture(b, [&](cudaStream_t c) { W::body(b, L, pl.bounces, pl.bounded, c); }, &b->exec,
+                                   "graph capture of a batch wave");
+            if (rc != LMGPU_OK) return rc;
             b->key = key;
         }
     }
@@ -510,18 +654,17 @@ int run_waves(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_t&
         LMGPU_CUDA_TRY(cudaGetLastError());
         if (pl.bounded) continue;
         // Unbounded depth: finish the wave's remaining bounces directly.
-        int k = pl.bounces + 1;
-        int slot = (TECH != LMGPU_RENDER_PT ? 1 : 0);   // counters reused: clear before each launch
-        for (;; k++) {
+        const int slot = (TECH != LMGPU_RENDER_PT ? 1 : 0);   // counters reused: clear before each launch
+        for (int k = pl.bounces + 1;; k++) {
             const int qin = (k - 1) & 1;
-            LMGPU_CUDA_TRY(cudaMemcpyAsync(b->h_counts, b->st.counters, 16, cudaMemcpyDeviceToHost, s));
+            LMGPU_CUDA_TRY(cudaMemcpyAsync(b->h_counts, b->st[0].counters, 16, cudaMemcpyDeviceToHost, s));
             LMGPU_CUDA_TRY(cudaStreamSynchronize(s));
             if (b->h_counts[qin] == 0) break;
             LMGPU_CUDA_TRY(cudaMemsetAsync(b->d_work + slot, 0, 2 * sizeof(unsigned long long), s));
-            W::bounce(b, L, k, qin, slot, s);
+            W::bounce(b, L, 0, k, slot, s);
             LMGPU_CUDA_TRY(cudaGetLastError());
         }
-        W::tail_end(b, L, s);
+        W::tail_end(b, L, 0, s);
         LMGPU_CUDA_TRY(cudaGetLastError());
     }
     return LMGPU_OK;
@@ -557,7 +700,10 @@ int check_config(const LmgpuBatchConfig& c)
         return fail(LMGPU_ERR_INVALID, "batch layout must be LMGPU_LAYOUT_BVH2 or LMGPU_LAYOUT_BVH4");
     if (c.wave_paths < 1024 || c.wave_paths > (1 << 26)) return fail(LMGPU_ERR_INVALID, "wave_paths must be in [1024, 2^26]");
     if (c.shade_blocks_per_sm < 1 || c.shade_blocks_per_sm > 64) return fail(LMGPU_ERR_INVALID, "shade_blocks_per_sm must be in [1, 64]");
-    if (c.mode != LMGPU_BATCH_WAVES && c.mode != LMGPU_BATCH_STREAM) return fail(LMGPU_ERR_INVALID, "unknown batch mode");
+    if (c.mode != LMGPU_BATCH_WAVES && c.mode != LMGPU_BATCH_STREAM && c.mode != LMGPU_BATCH_OVERLAP)
+        return fail(LMGPU_ERR_INVALID, "unknown batch mode");
+    if (c.overlap_bounce < 0 || c.overlap_bounce > MAX_BOUNDED_BOUNCES)
+        return fail(LMGPU_ERR_INVALID, "overlap_bounce must be in [0, 64]");
     return LMGPU_OK;
 }
 
@@ -573,11 +719,12 @@ int batch_render(LmgpuBatch* b, const LmgpuRenderParams* params, void* const* fi
     LMGPU_CUDA_TRY(cudaGetDevice(&cur));
     if (cur != b->device) return fail(LMGPU_ERR_INVALID, "batch used on another device than it was created on");
     int64_t P = std::min<int64_t>(b->cfg.wave_paths, pl.total);
-    rc = ensure_batch_workspace(b, std::max<int64_t>(P, b->ws_capacity));
+    const int pools = (b->cfg.mode == LMGPU_BATCH_OVERLAP && pl.bounded) ? 2 : 1;
+    rc = ensure_batch_workspace(b, std::max<int64_t>(P, b->ws_capacity), pools);
     // A device short of memory gets smaller waves (the configuration stays).
     while (rc == LMGPU_ERR_OOM && P > (int64_t(1) << 20)) {
         P /= 2;
-        rc = ensure_batch_workspace(b, P);
+        rc = ensure_batch_workspace(b, P, pools);
     }
     if (rc != LMGPU_OK) return rc;
     if ((rc = upload_table(b, params, films, s)) != LMGPU_OK) return rc;
@@ -642,11 +789,11 @@ int lmgpu_batch_create(LmgpuScene* const* scenes, int32_t num_scenes, LmgpuBatch
     auto hm = [&](void** p, size_t bytes) { if (e == cudaSuccess) e = cudaMallocHost(p, bytes); };
     dm(reinterpret_cast<void**>(&b->d_table), n * sizeof(BatchEntry));
     dm(reinterpret_cast<void**>(&b->d_begins), (n + 1) * sizeof(int64_t));
-    dm(reinterpret_cast<void**>(&b->d_wave), sizeof(WaveCtl));
+    dm(reinterpret_cast<void**>(&b->d_wave), POOLS * sizeof(WaveCtl));
     dm(reinterpret_cast<void**>(&b->d_ctl), sizeof(StreamCtl));
     hm(reinterpret_cast<void**>(&b->h_done), 2 * sizeof(int64_t));
     dm(reinterpret_cast<void**>(&b->d_stats), NSTATS * sizeof(unsigned long long));
-    dm(reinterpret_cast<void**>(&b->d_work), WORK_SLOTS * sizeof(unsigned long long));
+    dm(reinterpret_cast<void**>(&b->d_work), POOLS * WORK_SLOTS * sizeof(unsigned long long));
     dm(reinterpret_cast<void**>(&b->d_status), sizeof(int32_t));
     hm(reinterpret_cast<void**>(&b->h_table), n * sizeof(BatchEntry));
     hm(reinterpret_cast<void**>(&b->h_begins), (n + 1) * sizeof(int64_t));
@@ -654,6 +801,14 @@ int lmgpu_batch_create(LmgpuScene* const* scenes, int32_t num_scenes, LmgpuBatch
     hm(reinterpret_cast<void**>(&b->h_counts), 16);
     if (e == cudaSuccess) e = cudaMemset(b->d_status, 0, sizeof(int32_t));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
+    int least = 0, greatest = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&b->cap_hi, cudaStreamNonBlocking, greatest);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&b->cap_lo, cudaStreamNonBlocking, least);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&b->hi, cudaStreamNonBlocking, greatest);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&b->lo, cudaStreamNonBlocking, least);
+    for (cudaEvent_t& ev : b->ev)
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->staged, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         lmgpu_batch_destroy(b);
@@ -666,8 +821,12 @@ int lmgpu_batch_create(LmgpuScene* const* scenes, int32_t num_scenes, LmgpuBatch
 int lmgpu_batch_destroy(LmgpuBatch* b)
 {
     if (!b) return LMGPU_OK;
-    if (b->exec) cudaGraphExecDestroy(b->exec);
+    drop_graphs(b);
     if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+    for (cudaStream_t st : { b->cap_hi, b->cap_lo, b->hi, b->lo })
+        if (st) cudaStreamDestroy(st);
+    for (cudaEvent_t ev : b->ev)
+        if (ev) cudaEventDestroy(ev);
     if (b->staged) cudaEventDestroy(b->staged);
     cudaFree(b->ws_mem);
     cudaFree(b->d_table);
@@ -753,8 +912,9 @@ int lmgpu_batch_autotune(LmgpuBatch* b, const LmgpuRenderParams* params, double 
     best.use_graph = 1;
     double best_t = 1e30;
     rc = trial(best, best_t);
-    // Coordinate descent: mode, layout, then paths in flight, then shading grid.
-    for (int m : { LMGPU_BATCH_WAVES, LMGPU_BATCH_STREAM }) {
+    // Coordinate descent: mode, layout, then paths in flight, shading grid
+    // and (overlap mode) the first tail bounce.
+    for (int m : { LMGPU_BATCH_WAVES, LMGPU_BATCH_STREAM, LMGPU_BATCH_OVERLAP }) {
         if (rc != LMGPU_OK || m == best.mode) continue;
         LmgpuBatchConfig c = best;
         c.mode = m;
@@ -787,6 +947,16 @@ int lmgpu_batch_autotune(LmgpuBatch* b, const LmgpuRenderParams* params, double 
         c.shade_blocks_per_sm = g;
         double t;
         if ((rc = trial(c, t)) == LMGPU_OK && t < best_t) { best = c; best_t = t; }
+    }
+    if (best.mode == LMGPU_BATCH_OVERLAP) {
+        const int current = best.overlap_bounce > 0 ? best.overlap_bounce : DEFAULT_OVERLAP_BOUNCE;
+        for (int t0 : { 2, 3, 4, 5 }) {
+            if (rc != LMGPU_OK || t0 == current) continue;
+            LmgpuBatchConfig c = best;
+            c.overlap_bounce = t0;
+            double t;
+            if ((rc = trial(c, t)) == LMGPU_OK && t < best_t) { best = c; best_t = t; }
+        }
     }
     cudaFree(film);
     b->cfg = rc == LMGPU_OK ? best : start;

@@ -117,6 +117,7 @@ struct WaveCtl {
     int64_t count;         // paths in this wave
     int64_t total;         // samples of the whole batch
     int64_t step;          // wave capacity
+    int64_t stride;        // samples between this pool's consecutive waves (step × pools)
 };
 
 template <class F>

@@ -95,12 +95,12 @@ class RenderStats(ctypes.Structure):
                 ("waves", c_int32), ("max_bounces_run", c_int32), ("device_ms", c_double)]
 
 
-BATCH_WAVES, BATCH_STREAM = 0, 1
+BATCH_WAVES, BATCH_STREAM, BATCH_OVERLAP = 0, 1, 2
 
 
 class BatchConfig(ctypes.Structure):
     _fields_ = [("layout", c_int32), ("wave_paths", c_int32), ("shade_blocks_per_sm", c_int32),
-                ("use_graph", c_int32), ("mode", c_int32)]
+                ("use_graph", c_int32), ("mode", c_int32), ("overlap_bounce", c_int32)]
 
 
 # Every symbol include/lmgpu.h declares, with (restype, argtypes).

@@ -1,7 +1,7 @@
 """Multi-scene batch (lmgpu_batch_*): every scene of a batch must render the
 same paths as the one-scene renderer with the same parameters, whatever the
-batch configuration (BVH layout, wave size, shading grid, CUDA graph or
-direct launches). With FP64 films the two differ only in the order of the
+batch configuration (mode, BVH layout, wave size, shading grid, overlap
+bounce, CUDA graph or direct launches). With FP64 films the two differ only in the order of the
 film additions, so they agree to ~1e-12 relative.
 """
 import ctypes
@@ -88,13 +88,19 @@ def test_batch_matches_one_scene_renders(cuda, technique):
 
 @pytest.mark.parametrize("config", [
     dict(layout="qbvh"),
-    dict(wave_paths=4096),                       # stream: slots recycled many times, across scenes
+    dict(wave_paths=4096),                       # many waves, every wave spans scenes
     dict(wave_paths=1 << 20, shade_blocks_per_sm=2),
     dict(use_graph=False),
     dict(layout="qbvh", wave_paths=10000, use_graph=False),
     dict(mode="waves"),
     dict(mode="waves", wave_paths=4096),         # many waves, every wave spans scenes
     dict(mode="waves", layout="qbvh", wave_paths=10000, use_graph=False),
+    dict(mode="stream", wave_paths=4096),        # slots recycled many times, across scenes
+    dict(mode="overlap"),                        # one wave: head, no period, tail
+    dict(mode="overlap", wave_paths=4096),       # many waves in both pools
+    dict(mode="overlap", wave_paths=5000, overlap_bounce=1),    # the whole path loop is the tail
+    dict(mode="overlap", wave_paths=6000, overlap_bounce=12),   # split past the last bounce
+    dict(mode="overlap", layout="qbvh", wave_paths=4096, overlap_bounce=4, use_graph=False),  # two streams
 ])
 def test_batch_configurations_agree(cuda, config):
     items = small_set()
@@ -107,11 +113,12 @@ def test_batch_configurations_agree(cuda, config):
     batch.close()
 
 
-@pytest.mark.parametrize("mode", ["waves", "stream"])
+@pytest.mark.parametrize("mode", ["waves", "stream", "overlap"])
 def test_batch_unbounded_depth_tail(cuda, mode):
     """max_path_vertices = -1 (Russian roulette only): in wave mode the graph
-    covers the first bounces and direct launches finish the deep tail; in
-    stream mode every path simply lives until it ends."""
+    covers the first bounces and direct launches finish the deep tail
+    (overlap mode runs such renders as waves); in stream mode every path
+    simply lives until it ends."""
     items = [(scenes.cornell_box(32, 32, variant="mixed"), renderer("pt.mis", 1, -1, 5), 32 * 32 * 32),
              (scenes.cornell_box(24, 24), renderer("pt.mis", 1, -1, 6), 24 * 24 * 16)]
     built = [build(p) for p, _, _ in items]
@@ -122,21 +129,22 @@ def test_batch_unbounded_depth_tail(cuda, mode):
     batch.close()
 
 
-def test_stream_mode_statistics(cuda):
-    """Stream mode counts the same rays as wave mode (same paths) and reports
-    its iterations."""
+def test_mode_statistics(cuda):
+    """Stream and overlap modes count the same rays as wave mode (same
+    paths); stream mode reports its iterations, overlap mode its waves."""
     items = small_set()
     built = [build(p) for p, _, _ in items]
     batch = SceneBatch(built)
     stats = {}
-    for mode in ("waves", "stream"):
+    for mode in ("waves", "stream", "overlap"):
         batch.configure(mode=mode, wave_paths=8192)
         batch_films(batch, items)
         stats[mode] = dict(batch.last_stats)
-    assert stats["stream"]["rays_traced"] == stats["waves"]["rays_traced"]
-    assert stats["stream"]["shadow_rays"] == stats["waves"]["shadow_rays"]
-    assert stats["stream"]["max_bounces_run"] == stats["waves"]["max_bounces_run"]
+    for mode in ("stream", "overlap"):
+        for k in ("rays_traced", "shadow_rays", "max_bounces_run", "paths"):
+            assert stats[mode][k] == stats["waves"][k], (mode, k)
     assert stats["stream"]["waves"] > 8     # iterations
+    assert stats["overlap"]["waves"] == stats["waves"]["waves"] == -(-stats["waves"]["paths"] // 8192)
     batch.close()
 
 
@@ -164,7 +172,8 @@ def test_batch_autotune_keeps_results(cuda):
     want = plain_films(built, items)
     batch = SceneBatch(built)
     cfg = batch.autotune([r for _, r, _ in items], [n for _, _, n in items], sample_fraction=0.25)
-    assert cfg["layout"] in ("bvh", "qbvh") and cfg["trial_ms"] > 0 and cfg["mode"] in ("waves", "stream")
+    assert cfg["layout"] in ("bvh", "qbvh") and cfg["trial_ms"] > 0 and cfg["mode"] in ("waves", "stream", "overlap")
+    assert 0 <= cfg["overlap_bounce"] <= 5
     assert cfg["wave_paths"] in (1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25)
     assert_same(batch_films(batch, items), want)
     batch.close()
@@ -201,6 +210,10 @@ def test_batch_errors(cuda):
     assert L.lmgpu_batch_render_device(batch.handle, p, ptrs, None, None) == native.ERR_INVALID
     with pytest.raises(native.LmgpuError):
         batch.configure(wave_paths=16)
+    with pytest.raises(native.LmgpuError):
+        batch.configure(mode="overlap", overlap_bounce=65)
+    with pytest.raises(ValueError):
+        batch.configure(mode="pipelined")
     with pytest.raises(ValueError):
         batch.configure(layout="naive")
     batch.close()
