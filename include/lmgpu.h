@@ -327,10 +327,13 @@ int lmgpu_batch_render_device(LmgpuBatch* batch, const LmgpuRenderParams* params
                               void* const* films_device, void* stream, LmgpuRenderStats* stats);
 
 /* Autotuner: renders the batch with each scene's sample count scaled by
- * `sample_fraction` (0 < f <= 1) under candidate configurations (mode, BVH
- * layout, paths in flight, shading grid, overlap bounce), coordinate by coordinate, keeps the
- * fastest, stores it as the batch's configuration and returns it with its
- * device time in ms. Films are scratch memory of the tuner; synchronises. */
+ * `sample_fraction` (0 < f <= 1; raised for a candidate until the trial
+ * holds four of its waves, or the whole render) under candidate
+ * configurations (mode, BVH layout, paths in flight, shading grid, overlap
+ * bounce), coordinate by coordinate, keeps the one with the least device
+ * time per sample, stores it as the batch's configuration and returns it
+ * with that time scaled to `sample_fraction` of the samples, in ms. Films
+ * are scratch memory of the tuner; synchronises. */
 int lmgpu_batch_autotune(LmgpuBatch* batch, const LmgpuRenderParams* params, double sample_fraction,
                          void* stream, LmgpuBatchConfig* chosen, double* best_ms);
 

@@ -124,7 +124,9 @@ class SceneBatch:
 
     def autotune(self, renderers, num_samples, sample_fraction: float = 0.125, stream=None) -> dict:
         """Chooses mode, layout, wave size, shading grid and overlap bounce by timing scaled-down
-        renders of this batch; the choice becomes the batch's configuration."""
+        renders of this batch (each candidate on at least four of its waves, or
+        the whole render; compared by time per sample); the choice becomes the
+        batch's configuration. trial_ms is the winner's time at sample_fraction."""
         import torch
         params = self._params(renderers, num_samples, False)
         s = stream if stream is not None else torch.cuda.current_stream().cuda_stream

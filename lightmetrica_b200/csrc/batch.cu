@@ -878,12 +878,20 @@ int lmgpu_batch_autotune(LmgpuBatch* b, const LmgpuRenderParams* params, double 
     const size_t n = b->scenes.size();
     // Scaled budgets, one scratch film shared by all scenes (its contents are discarded).
     std::vector<LmgpuRenderParams> p(params, params + n);
-    int64_t px = 0, total = 0;
+    auto scale = [&](double f) {
+        int64_t t = 0;
+        for (size_t i = 0; i < n; i++) {
+            p[i].num_samples = std::max<int64_t>(1, (int64_t)std::llround((double)params[i].num_samples * f));
+            t += p[i].num_samples;
+        }
+        return t;
+    };
+    int64_t px = 0, full = 0;
     for (size_t i = 0; i < n; i++) {
-        p[i].num_samples = std::max<int64_t>(1, (int64_t)std::llround((double)params[i].num_samples * fraction));
-        total += p[i].num_samples;
+        full += params[i].num_samples;
         px = std::max<int64_t>(px, (int64_t)b->scenes[i]->dev.cam.width * b->scenes[i]->dev.cam.height);
     }
+    const int64_t total = scale(fraction);
     Plan pl;
     int rc = make_plan(b, p.data(), nullptr, pl);
     if (rc != LMGPU_OK) return rc;
@@ -893,11 +901,16 @@ int lmgpu_batch_autotune(LmgpuBatch* b, const LmgpuRenderParams* params, double 
     std::vector<void*> films(n, film);
 
     const LmgpuBatchConfig start = b->cfg;
-    auto trial = [&](const LmgpuBatchConfig& c, double& ms) -> int {
+    // A candidate is timed on at least four of its own waves (or the whole
+    // render), so that large waves are not judged on a render that one wave
+    // holds, and is compared by device time per sample.
+    auto trial = [&](const LmgpuBatchConfig& c, double& ms_per_sample) -> int {
         int r = check_config(c);
         if (r != LMGPU_OK) return r;
-        ms = 1e30;
+        ms_per_sample = 1e30;
         b->cfg = c;
+        const double f = std::min(1.0, std::max(fraction, 4.0 * (double)c.wave_paths / (double)full));
+        const int64_t samples = scale(f);
         LmgpuRenderStats st;
         if ((r = batch_render(b, p.data(), films.data(), s, &st)) != LMGPU_OK) return r;   // warm-up (capture)
         double best = 1e30;
@@ -905,7 +918,7 @@ int lmgpu_batch_autotune(LmgpuBatch* b, const LmgpuRenderParams* params, double 
             if ((r = batch_render(b, p.data(), films.data(), s, &st)) != LMGPU_OK) return r;
             best = std::min(best, st.device_ms);
         }
-        ms = best;
+        ms_per_sample = best / (double)samples;
         return LMGPU_OK;
     };
     LmgpuBatchConfig best = start;
@@ -934,7 +947,7 @@ int lmgpu_batch_autotune(LmgpuBatch* b, const LmgpuRenderParams* params, double 
     int64_t largest = 0;
     for (int w : waves) {
         // Waves beyond the sample count behave like a wave of the sample count.
-        if (rc != LMGPU_OK || w == best.wave_paths || (w > total && largest >= total)) continue;
+        if (rc != LMGPU_OK || w == best.wave_paths || (w > full && largest >= full)) continue;
         largest = std::max<int64_t>(largest, w);
         LmgpuBatchConfig c = best;
         c.wave_paths = w;
@@ -962,7 +975,7 @@ int lmgpu_batch_autotune(LmgpuBatch* b, const LmgpuRenderParams* params, double 
     b->cfg = rc == LMGPU_OK ? best : start;
     if (rc != LMGPU_OK) return rc;
     if (chosen) *chosen = best;
-    if (best_ms) *best_ms = best_t;
+    if (best_ms) *best_ms = best_t * (double)total;
     return LMGPU_OK;
 }
 
