@@ -219,7 +219,7 @@ int lmgpu_render(LmgpuScene* scene, const LmgpuRenderParams* params,
  * (float, or double when film_fp64) on `stream`; the caller rescales by
  * W*H/num_samples. The call returns once the render's device work is done
  * (it reads each bounce's queue sizes back to size the next launch). Waves
- * hold `wave_paths` paths (0 = 2^24, fewer if device memory is short) in a
+ * hold `wave_paths` paths (0 = 2^25, fewer if device memory is short) in a
  * workspace of about 176 bytes per path that is shared by all scenes of the
  * device and kept until exit; calls on one device take turns. */
 int lmgpu_render_device(LmgpuScene* scene, const LmgpuRenderParams* params,
@@ -308,7 +308,7 @@ typedef struct LmgpuBatchConfig {
 
 /* The scenes (built with a BVH layout, on the current device) must outlive
  * the batch; a scene may appear more than once. Default configuration:
- * BVH2, 2^24 paths in flight (about 3 GB of path state), 16 shading blocks
+ * BVH2, 2^25 paths in flight (about 8 GB of path state), 16 shading blocks
  * per SM, graphs on, fixed waves (stream mode keeps every slot busy, but its
  * recycled slots scatter path state in memory: slower on the benchmark
  * scenes); a device short of memory gets fewer paths in flight. */

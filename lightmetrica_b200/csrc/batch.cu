@@ -73,7 +73,7 @@ struct LmgpuBatch {
     int device = 0;
     int sms = 148;
     std::vector<LmgpuScene*> scenes;
-    LmgpuBatchConfig cfg{ LMGPU_LAYOUT_BVH2, 1 << 24, 16, 1, LMGPU_BATCH_WAVES, 0 };
+    LmgpuBatchConfig cfg{ LMGPU_LAYOUT_BVH2, 1 << 25, 16, 1, LMGPU_BATCH_WAVES, 0 };
 
     BatchEntry* d_table = nullptr;
     int64_t* d_begins = nullptr;
