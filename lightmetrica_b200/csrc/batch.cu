@@ -568,25 +568,28 @@ int run_overlap(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_
 
     auto head0 = [&](cudaStream_t a) { W::head(b, L, 0, T, a); };
     auto tail0 = [&](cudaStream_t a) { W::tail(b, L, 0, T, K, a); };
-    // Event calls inside a capture fail only with the capture, which the
-    // capture's end reports; for direct launches they are checked after.
-    auto period = [&](cudaStream_t a, cudaStream_t hi, cudaStream_t lo) {
+    // Returns the first failing event call (inside a capture, the capture's
+    // end reports it too).
+    auto period = [&](cudaStream_t a, cudaStream_t hi, cudaStream_t lo) -> cudaError_t {
         cudaEvent_t* ev = b->ev;
-        cudaEventRecord(ev[0], a);
-        cudaStreamWaitEvent(hi, ev[0], 0);
-        cudaStreamWaitEvent(lo, ev[0], 0);
+        cudaError_t e = cudaSuccess;
+        auto chk = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+        chk(cudaEventRecord(ev[0], a));
+        chk(cudaStreamWaitEvent(hi, ev[0], 0));
+        chk(cudaStreamWaitEvent(lo, ev[0], 0));
         W::tail(b, L, 0, T, K, lo);
-        cudaEventRecord(ev[1], lo);
+        chk(cudaEventRecord(ev[1], lo));
         W::head(b, L, 1, T, hi);
-        cudaEventRecord(ev[2], hi);
-        cudaStreamWaitEvent(hi, ev[1], 0);
+        chk(cudaEventRecord(ev[2], hi));
+        chk(cudaStreamWaitEvent(hi, ev[1], 0));
         W::head(b, L, 0, T, hi);
-        cudaEventRecord(ev[3], hi);
-        cudaStreamWaitEvent(lo, ev[2], 0);
+        chk(cudaEventRecord(ev[3], hi));
+        chk(cudaStreamWaitEvent(lo, ev[2], 0));
         W::tail(b, L, 1, T, K, lo);
-        cudaEventRecord(ev[4], lo);
-        cudaStreamWaitEvent(a, ev[3], 0);
-        cudaStreamWaitEvent(a, ev[4], 0);
+        chk(cudaEventRecord(ev[4], lo));
+        chk(cudaStreamWaitEvent(a, ev[3], 0));
+        chk(cudaStreamWaitEvent(a, ev[4], 0));
+        return e;
     };
     if (b->cfg.use_graph) {
         GraphKey key;
@@ -597,7 +600,7 @@ int run_overlap(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_
             drop_graphs(b);
             int rc = capture(b, head0, &b->exec_head, "graph capture of a wave head");
             if (rc == LMGPU_OK)
-                rc = capture(b, [&](cudaStream_t a) { period(a, b->cap_hi, b->cap_lo); }, &b->exec,
+                rc = capture(b, [&](cudaStream_t a) { (void)period(a, b->cap_hi, b->cap_lo); }, &b->exec,
                              "graph capture of an overlap period", cudaGraphInstantiateFlagUseNodePriority);
             if (rc == LMGPU_OK) rc = capture(b, tail0, &b->exec_tail, "graph capture of a wave tail");
             if (rc != LMGPU_OK) { drop_graphs(b); return rc; }
@@ -611,8 +614,15 @@ int run_overlap(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_
     head0(s);
     LMGPU_CUDA_TRY(cudaGetLastError());
     for (int64_t j = 0; j < periods; j++) {
-        period(s, b->hi, b->lo);
-        LMGPU_CUDA_TRY(cudaGetLastError());
+        cudaError_t e = period(s, b->hi, b->lo);
+        if (e == cudaSuccess) e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            // Nothing of this render may still run on the branch streams
+            // once the call has returned.
+            cudaStreamSynchronize(b->hi);
+            cudaStreamSynchronize(b->lo);
+            return cuda_fail(e, "overlap period (direct launches)");
+        }
     }
     tail0(s);
     LMGPU_CUDA_TRY(cudaGetLastError());
