@@ -337,6 +337,55 @@ int lmgpu_batch_render_device(LmgpuBatch* batch, const LmgpuRenderParams* params
 int lmgpu_batch_autotune(LmgpuBatch* batch, const LmgpuRenderParams* params, double sample_fraction,
                          void* stream, LmgpuBatchConfig* chosen, double* best_ms);
 
+/* ------------------------------------------------ component evaluation ---- */
+/* The path tracer's own device functions for caller-given inputs (host
+ * arrays in and out; each call allocates scratch device memory and
+ * synchronises: utility calls for checks and tools, not a hot path). They
+ * answer what the reference's components answer for one query:
+ *   lmgpu_eval_sampling          Math::UniformConcentricDiskSample /
+ *                                CosineSampleHemisphere (math.stats.inl:25-69)
+ *   lmgpu_camera_sample_rays     PerspectiveCamera::SamplePosition +
+ *                                SampleDirection (perspectivecamera.cpp:170-240)
+ *   lmgpu_camera_raster_positions  PerspectiveCamera::RayToRasterPosition
+ *                                (perspectivecamera.cpp:304-323)
+ *   lmgpu_film_pixels            the pixel HDRBitmapFilm::AccumulateContribution
+ *                                adds a raster position to (hdrfilm.cpp:151-171)
+ *   lmgpu_bsdf_sample            BSDF::SampleAndEstimateDirection, transport
+ *                                EL (diffuse.cpp:133-157, mirror.cpp:84-107,
+ *                                diffusemirror.cpp:84-125)
+ *   lmgpu_bsdf_evaluate          BSDF::EvaluateDirection / EvaluateDirectionPDF
+ *                                for a NonDelta query (diffuse.cpp:192-220)
+ * Counts are in [0, 2^30]. */
+enum {
+    LMGPU_EVAL_CONCENTRIC_DISK = 0,     /* u (n x 2) -> point on the unit disk (n x 2) */
+    LMGPU_EVAL_COSINE_HEMISPHERE = 1    /* u (n x 2) -> direction, +z hemisphere (n x 3) */
+};
+int lmgpu_eval_sampling(int32_t fn, const float* u, int64_t n, float* out);
+
+/* The scene's camera: raster positions in [0,1]^2 (n x 2; y = 0 is the
+ * bottom row) -> ray origin and direction (n x 6) and the importance pdf
+ * (n, projected solid angle). */
+int lmgpu_camera_sample_rays(const LmgpuScene* scene, const float* raster, int64_t n, float* rays, float* pdf);
+/* Rays (n x 6: origin, direction) -> raster positions (n x 2) and valid (n;
+ * 0 when the direction leaves the film). */
+int lmgpu_camera_raster_positions(const LmgpuScene* scene, const float* rays, int64_t n, float* raster,
+                                  int32_t* valid);
+/* Raster positions (n x 2) -> pixel index y * W + x of the scene camera's
+ * film (n; -1 outside [0,1]^2), as the renderers' film splats map them. */
+int lmgpu_film_pixels(const LmgpuScene* scene, const float* raster, int64_t n, int32_t* pixel);
+
+/* BSDF `type` (LMGPU_BSDF_*) with reflectance R (3 floats) at frames given by
+ * geometric and shading normals (n x 6: gn, sn; tangents from sn as
+ * SurfaceGeometry::ComputeTangentSpace makes them), for wi (n x 3, towards the
+ * previous vertex) and u (n x 3: direction sample, component sample):
+ * sampled wo (n x 3), weight f cos / pdf (n x 3), pdf (n, projected solid
+ * angle) and specular (n, optional). */
+int lmgpu_bsdf_sample(int32_t type, const float* reflectance, const float* frames, const float* wi, const float* u,
+                      int64_t n, float* wo, float* weight, float* pdf, int32_t* specular);
+/* f (n x 3) and pdf (n) of the non-delta part for wi, wo (n x 3 each). */
+int lmgpu_bsdf_evaluate(int32_t type, const float* reflectance, const float* frames, const float* wi, const float* wo,
+                        int64_t n, float* f, float* pdf);
+
 /* ------------------------------------------------------------- misc ----- */
 const char* lmgpu_last_error(void);
 int lmgpu_abi_version(void);

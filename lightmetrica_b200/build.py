@@ -21,7 +21,7 @@ OUT_DIR = os.path.join(HERE, "_lib")
 OUT = os.path.join(OUT_DIR, "liblmgpu.so")
 BUILD_DIR = os.path.join(HERE, "_build")
 
-CU_SOURCES = ["api.cu", "pathtrace.cu", "adjoint.cu", "noalloc.cu", "batch.cu"]
+CU_SOURCES = ["api.cu", "pathtrace.cu", "adjoint.cu", "noalloc.cu", "batch.cu", "eval.cu"]
 CPP_SOURCES = ["builder.cpp"]
 HEADERS = ["layout.h", "builder.h", "internal.h", "scene.cuh", "trace.cuh", "trace4.cuh",
            "shading.cuh", "rng.cuh", "pathtrace.cuh", "trace_kernels.cuh", "pt_kernels.cuh"]

@@ -96,6 +96,7 @@ class RenderStats(ctypes.Structure):
 
 
 BATCH_WAVES, BATCH_STREAM, BATCH_OVERLAP = 0, 1, 2
+EVAL_CONCENTRIC_DISK, EVAL_COSINE_HEMISPHERE = 0, 1
 
 
 class BatchConfig(ctypes.Structure):
@@ -130,6 +131,13 @@ SIGNATURES = {
     "lmgpu_batch_render_device": (c_int32, [c_void_p, P(RenderParams), P(c_void_p), c_void_p, P(RenderStats)]),
     "lmgpu_batch_autotune": (c_int32, [c_void_p, P(RenderParams), c_double, c_void_p, P(BatchConfig),
                                        P(c_double)]),
+    "lmgpu_eval_sampling": (c_int32, [c_int32, c_void_p, c_int64, c_void_p]),
+    "lmgpu_camera_sample_rays": (c_int32, [c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
+    "lmgpu_camera_raster_positions": (c_int32, [c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
+    "lmgpu_film_pixels": (c_int32, [c_void_p, c_void_p, c_int64, c_void_p]),
+    "lmgpu_bsdf_sample": (c_int32, [c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p,
+                                    c_void_p, c_void_p]),
+    "lmgpu_bsdf_evaluate": (c_int32, [c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
 }
 
 _lib = None

@@ -82,6 +82,55 @@ class HDRBitmapFilm:
             self.data = np.zeros((self.height, self.width, 3), np.float32)
         return self.data
 
+    def allocate(self, width: int, height: int) -> None:
+        """HDRBitmapFilm::Allocate (hdrfilm.cpp:327-332): zeroed W x H."""
+        self.width, self.height = int(width), int(height)
+        self.data = np.zeros((self.height, self.width, 3), np.float32)
+
+    def pixel_of(self, raster) -> int:
+        """Pixel index of a raster position in [0,1]^2, or -1 outside it:
+        int(r * W) in float arithmetic, clamped to the film
+        (hdrfilm.cpp:151-163)."""
+        rx, ry = np.float32(raster[0]), np.float32(raster[1])
+        if rx < 0 or rx > 1 or ry < 0 or ry > 1:
+            return -1
+        x = min(max(int(rx * np.float32(self.width)), 0), self.width - 1)
+        y = min(max(int(ry * np.float32(self.height)), 0), self.height - 1)
+        return y * self.width + x
+
+    def record_contribution(self, raster, contribution) -> bool:
+        """HDRBitmapFilm::RecordContribution (hdrfilm.cpp:129-149): sets the pixel."""
+        i = self.pixel_of(raster)
+        if i < 0:
+            return False
+        self.internal_data().reshape(-1, 3)[i] = np.asarray(contribution, np.float32)
+        return True
+
+    def accumulate_contribution(self, raster, contribution) -> bool:
+        """HDRBitmapFilm::AccumulateContribution(rasterPos, contrb)
+        (hdrfilm.cpp:151-171): adds to the pixel; a position outside [0,1]^2
+        is ignored (the reference logs a warning)."""
+        i = self.pixel_of(raster)
+        if i < 0:
+            return False
+        self.internal_data().reshape(-1, 3)[i] += np.asarray(contribution, np.float32)
+        return True
+
+    def accumulate_film(self, other: "HDRBitmapFilm") -> bool:
+        """HDRBitmapFilm::AccumulateContribution(film) (hdrfilm.cpp:173-197):
+        adds another film of the same size (else ignored, as the reference)."""
+        if other.width != self.width or other.height != self.height:
+            return False
+        self.internal_data()[...] += other.internal_data()
+        return True
+
+    def rescale(self, weight: float) -> None:
+        """HDRBitmapFilm::Rescale (hdrfilm.cpp:334-341)."""
+        self.internal_data()[...] *= np.float32(weight)
+
+    def clone(self) -> "HDRBitmapFilm":
+        return HDRBitmapFilm(self.width, self.height, self.internal_data().copy(), self.image_type)
+
     def rescale_and_save(self, path: str, weight: float = 1.0) -> str:
         """HDRBitmapFilm::RescaleAndSave (hdrfilm.cpp:199-304); returns the
         path written (see film_io for the naming rules)."""

@@ -468,3 +468,98 @@ def oracle_grad(prims, dL_dimage, technique="pt.mis", spp=16, rr_depth=1, max_pa
         L.orc_render_grad(ctypes.byref(dd), g.ctypes.data, outs[0].ctypes.data, outs[1].ctypes.data)
     ga, gl = _split_run(run, d, total, threads, [np.zeros(3 * T), np.zeros(3 * nl)])
     return ga.reshape(T, 3), gl.reshape(nl, 3)[:d.num_lights]
+
+
+# ------------------------------------------------ component evaluation ----
+# The oracle's camera, sampling and BSDF functions (lmoracle_pt.c) for
+# given inputs, in float64.
+
+BSDF_TYPES = {"diffuse": 0, "mirror": 1, "diffuse_mirror": 2}
+
+
+def _components():
+    """liblmoracle with the component entry points' signatures declared."""
+    L = lib()
+    if not getattr(L, "_components_bound", False):
+        P, I = ctypes.c_void_p, ctypes.c_int
+        L.orc_eval_disk.argtypes = [P, I, P]
+        L.orc_eval_cosine.argtypes = [P, I, P]
+        L.orc_camera_rays.argtypes = [ctypes.POINTER(_OrcPtDesc), P, I, P, P]
+        L.orc_camera_rays.restype = I
+        L.orc_camera_raster.argtypes = [ctypes.POINTER(_OrcPtDesc), P, I, P, P]
+        L.orc_camera_raster.restype = I
+        L.orc_bsdf_sample.argtypes = [I, P, P, P, P, I, P, P, P, P]
+        L.orc_bsdf_eval.argtypes = [I, P, P, P, P, I, P, P]
+        L._components_bound = True
+    return L
+
+
+def _f64(a, cols):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1, cols))
+
+
+def eval_disk(u):
+    """UniformConcentricDiskSample of u (n x 2) -> (n x 2)."""
+    u = _f64(u, 2)
+    out = np.empty_like(u)
+    _components().orc_eval_disk(_ptr(u), u.shape[0], _ptr(out))
+    return out
+
+
+def eval_cosine(u):
+    """CosineSampleHemisphere of u (n x 2) -> (n x 3)."""
+    u = _f64(u, 2)
+    out = np.empty((u.shape[0], 3))
+    _components().orc_eval_cosine(_ptr(u), u.shape[0], _ptr(out))
+    return out
+
+
+def _camera_desc(eye, center, up, fovy, width, height):
+    d = _OrcPtDesc()
+    d.eye[:], d.center[:], d.up[:] = list(map(float, eye)), list(map(float, center)), list(map(float, up))
+    d.fovy, d.width, d.height = float(fovy), int(width), int(height)
+    return d
+
+
+def camera_rays(raster, eye, center, up, fovy, width, height):
+    """Raster positions (n x 2) -> (origins and directions (n x 6), pdf (n))."""
+    r = _f64(raster, 2)
+    rays, pdf = np.empty((r.shape[0], 6)), np.empty(r.shape[0])
+    d = _camera_desc(eye, center, up, fovy, width, height)
+    if not _components().orc_camera_rays(ctypes.byref(d), _ptr(r), r.shape[0], _ptr(rays), _ptr(pdf)):
+        raise ValueError("degenerate camera")
+    return rays, pdf
+
+
+def camera_raster(rays, eye, center, up, fovy, width, height):
+    """Rays (n x 6: origin, direction) -> (raster (n x 2), valid (n))."""
+    r = _f64(rays, 6)
+    raster, valid = np.empty((r.shape[0], 2)), np.empty(r.shape[0], dtype=np.int32)
+    d = _camera_desc(eye, center, up, fovy, width, height)
+    if not _components().orc_camera_raster(ctypes.byref(d), _ptr(r), r.shape[0], _ptr(raster), _ptr(valid)):
+        raise ValueError("degenerate camera")
+    return raster, valid.astype(bool)
+
+
+def bsdf_sample(bsdf, R, frames, wi, u):
+    """SampleAndEstimateDirection: frames (n x 6: gn, sn), wi (n x 3), u (n x 3)
+    -> dict of wo, weight (n x 3), pdf (n), specular (n)."""
+    f, w, uu = _f64(frames, 6), _f64(wi, 3), _f64(u, 3)
+    n = f.shape[0]
+    R = _f64(R, 3)
+    out = {"wo": np.empty((n, 3)), "weight": np.empty((n, 3)), "pdf": np.empty(n), "specular": np.empty(n, dtype=np.int32)}
+    _components().orc_bsdf_sample(BSDF_TYPES[bsdf], _ptr(R), _ptr(f), _ptr(w), _ptr(uu), n,
+                          _ptr(out["wo"]), _ptr(out["weight"]), _ptr(out["pdf"]), _ptr(out["specular"]))
+    out["specular"] = out["specular"].astype(bool)
+    return out
+
+
+def bsdf_eval(bsdf, R, frames, wi, wo):
+    """EvaluateDirection / EvaluateDirectionPDF (NonDelta): -> (f (n x 3), pdf (n))."""
+    f, a, b = _f64(frames, 6), _f64(wi, 3), _f64(wo, 3)
+    n = f.shape[0]
+    R = _f64(R, 3)
+    fs, pdf = np.empty((n, 3)), np.empty(n)
+    _components().orc_bsdf_eval(BSDF_TYPES[bsdf], _ptr(R), _ptr(f), _ptr(a), _ptr(b), n,
+                        _ptr(fs), _ptr(pdf))
+    return fs, pdf

@@ -740,3 +740,106 @@ int64_t orc_render_grad(const orc_pt_desc* d, const double* dL_dI, double* d_alb
     teardown(&s);
     return d->sample_end - d->sample_begin;
 }
+
+/* ------------------------------------------------ component evaluation -- */
+/* The camera, sampling and BSDF functions above for caller-given inputs:
+ * tests check them against the reference's component tests
+ * (test.math.stats.cpp:32-84, test.perspectivecamera.cpp:84-194,
+ * test.generalizedbsdf.cpp:129-268) and compare the device's versions with
+ * them. */
+
+/* UniformConcentricDiskSample: u (n x 2) -> points (n x 2). */
+void orc_eval_disk(const double* u, int n, double* out)
+{
+    for (int i = 0; i < n; i++) concentric(u[2 * i], u[2 * i + 1], &out[2 * i], &out[2 * i + 1]);
+}
+
+/* CosineSampleHemisphere (math.stats.inl:64-69): u (n x 2) -> directions (n x 3). */
+void orc_eval_cosine(const double* u, int n, double* out)
+{
+    for (int i = 0; i < n; i++) {
+        double x, y;
+        concentric(u[2 * i], u[2 * i + 1], &x, &y);
+        out[3 * i] = x;
+        out[3 * i + 1] = y;
+        out[3 * i + 2] = sqrt(fmax(0.0, 1 - x * x - y * y));
+    }
+}
+
+/* The camera of d (eye, center, up, fovy, width, height; no geometry is
+ * needed): raster positions (n x 2) -> ray origin and direction (n x 6) and
+ * the importance pdf (n). Returns 0 for a degenerate camera. */
+int orc_camera_rays(const orc_pt_desc* d, const double* raster, int n, double* rays, double* pdf)
+{
+    pt_scene s;
+    const int ok = setup(&s, d);
+    for (int i = 0; ok && i < n; i++) {
+        v3 w = cam_dir(&s, raster[2 * i], raster[2 * i + 1], &pdf[i]);
+        rays[6 * i] = s.cam_p.x; rays[6 * i + 1] = s.cam_p.y; rays[6 * i + 2] = s.cam_p.z;
+        rays[6 * i + 3] = w.x; rays[6 * i + 4] = w.y; rays[6 * i + 5] = w.z;
+    }
+    teardown(&s);
+    return ok;
+}
+
+/* RayToRasterPosition: rays (n x 6) -> raster (n x 2) and valid (n; 0 when
+ * the direction leaves the film). Returns 0 for a degenerate camera. */
+int orc_camera_raster(const orc_pt_desc* d, const double* rays, int n, double* raster, int* valid)
+{
+    pt_scene s;
+    const int ok = setup(&s, d);
+    for (int i = 0; ok && i < n; i++) {
+        double We;
+        const double* r = rays + 6 * i;
+        valid[i] = cam_project(&s, mk(r[0], r[1], r[2]), mk(r[3], r[4], r[5]), &raster[2 * i], &raster[2 * i + 1], &We);
+    }
+    teardown(&s);
+    return ok;
+}
+
+static geom frame_of(const double* gnsn)
+{
+    geom g;
+    memset(&g, 0, sizeof(g));
+    g.gn = mk(gnsn[0], gnsn[1], gnsn[2]);
+    g.sn = mk(gnsn[3], gnsn[4], gnsn[5]);
+    tangent(&g);
+    return g;
+}
+
+/* BSDF type (0 diffuse, 1 mirror, 2 diffuse-mirror) with reflectance R (3)
+ * at frames given by geometric and shading normals (n x 6; tangents from the
+ * shading normal, SurfaceGeometry::ComputeTangentSpace): SampleAndEstimate-
+ * Direction (EL) for wi (n x 3) and u (n x 3: sample, component) -> wo,
+ * weight (n x 3 each), pdf (n, projected solid angle) and specular (n). */
+void orc_bsdf_sample(int type, const double* R, const double* frames, const double* wi, const double* u, int n,
+                     double* wo, double* weight, double* pdf, int* spec)
+{
+    mat_t m;
+    m.type = type;
+    m.R = mk(R[0], R[1], R[2]);
+    for (int i = 0; i < n; i++) {
+        geom g = frame_of(frames + 6 * i);
+        v3 o = mk(0, 0, 1);
+        v3 w = bsdf_sample(&m, &g, mk(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]), u[3 * i], u[3 * i + 1], u[3 * i + 2],
+                           &o, &pdf[i], &spec[i]);
+        wo[3 * i] = o.x; wo[3 * i + 1] = o.y; wo[3 * i + 2] = o.z;
+        weight[3 * i] = w.x; weight[3 * i + 1] = w.y; weight[3 * i + 2] = w.z;
+    }
+}
+
+/* EvaluateDirection and EvaluateDirectionPDF for a NonDelta query (EL):
+ * wi, wo (n x 3) -> f (n x 3) and pdf (n). */
+void orc_bsdf_eval(int type, const double* R, const double* frames, const double* wi, const double* wo, int n,
+                   double* f, double* pdf)
+{
+    mat_t m;
+    m.type = type;
+    m.R = mk(R[0], R[1], R[2]);
+    for (int i = 0; i < n; i++) {
+        geom g = frame_of(frames + 6 * i);
+        v3 v = bsdf_eval(&m, &g, mk(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]), mk(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]),
+                         &pdf[i]);
+        f[3 * i] = v.x; f[3 * i + 1] = v.y; f[3 * i + 2] = v.z;
+    }
+}
