@@ -143,12 +143,14 @@ int copy_in(void* dst, const void* src, size_t bytes)
     return LMGPU_OK;
 }
 
+// Copies the outputs back (each copy waits for the kernel on the legacy
+// stream) and waits for that stream alone.
 int finish(void* const* dst, void* const* src, const size_t* bytes, int k)
 {
     LMGPU_CUDA_TRY(cudaGetLastError());
     for (int i = 0; i < k; i++)
         if (dst[i]) LMGPU_CUDA_TRY(cudaMemcpy(dst[i], src[i], bytes[i], cudaMemcpyDeviceToHost));
-    LMGPU_CUDA_TRY(cudaDeviceSynchronize());
+    LMGPU_CUDA_TRY(cudaStreamSynchronize(0));
     return LMGPU_OK;
 }
 
