@@ -221,7 +221,8 @@ class _RefRenderDesc(ctypes.Structure):
                 ("width", ctypes.c_int), ("height", ctypes.c_int), ("renderer", ctypes.c_char_p),
                 ("rr_depth", ctypes.c_int), ("max_path_vertices", ctypes.c_int), ("seed", ctypes.c_int),
                 ("num_samples", ctypes.c_longlong), ("num_threads", ctypes.c_int),
-                ("samples_per_block", ctypes.c_longlong), ("scene_type", ctypes.c_char_p)]
+                ("samples_per_block", ctypes.c_longlong), ("scene_type", ctypes.c_char_p),
+                ("sched_type", ctypes.c_char_p)]
 
 
 def flatten_primitives(prims):
@@ -268,11 +269,12 @@ def flatten_primitives(prims):
 
 
 def ref_render(prims, renderer="pt", num_samples=None, spp=16, rr_depth=1, max_path_vertices=-1, seed=1,
-               threads=None, precision="d", samples_per_block=100, scene_type="bvh"):
-    """Renders `prims` with the reference's own renderer + `mt` scheduler
-    (oracle/_ref) over the accelerator `scene_type` (the reference's "bvh",
-    or a loaded plugin's scene such as "plugin.gpu"). Returns (film (H, W, 3)
-    float32, render seconds)."""
+               threads=None, precision="d", samples_per_block=100, scene_type="bvh", sched_type="mt"):
+    """Renders `prims` with the reference's own component wiring (oracle/_ref):
+    renderer `renderer`, scheduler `sched_type` (the reference's "mt") and
+    accelerator `scene_type` (the reference's "bvh"); a loaded plugin's
+    components ("plugin.gpu", "gpu.pt.mis", "gpu") can take any of the three
+    slots. Returns (film (H, W, 3) float32, render seconds)."""
     L = ref(precision)
     if not hasattr(L, "lmref_render"):
         raise RuntimeError("reference harness built without the renderer")
@@ -323,11 +325,13 @@ def ref_render(prims, renderer="pt", num_samples=None, spp=16, rr_depth=1, max_p
     d.num_threads = int(threads or os.cpu_count() or 1)
     d.samples_per_block = samples_per_block
     d.scene_type = scene_type.encode()
+    d.sched_type = sched_type.encode()
     film = np.zeros((H, W, 3), np.float32)
     bt = ctypes.c_double()
     secs = L.lmref_render(ctypes.byref(d), film.ctypes.data, ctypes.byref(bt))
     if secs < 0:
-        raise RuntimeError(f"reference render failed ({secs})")
+        L.lmref_last_error.restype = ctypes.c_char_p
+        raise RuntimeError(f"reference render failed ({secs}): {L.lmref_last_error().decode(errors='replace')}")
     return film, secs
 
 

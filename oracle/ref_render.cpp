@@ -68,6 +68,7 @@ struct RefRenderDesc {
     int num_threads;
     long long samples_per_block;
     const char* scene_type;             // accelerator ("bvh" when null), e.g. a plugin's "plugin.gpu"
+    const char* sched_type;             // render process scheduler ("mt" when null), e.g. a plugin's "gpu"
 };
 }
 
@@ -298,7 +299,9 @@ double lmref_render(const RefRenderDesc* d, float* film_out, double* build_secon
     if (build_seconds) *build_seconds = std::chrono::duration<double>(tb1 - tb0).count();
 
     // Scheduler and renderer
-    std::unique_ptr<RenderProcessScheduler> sched(ComponentFactory::Create<RenderProcessScheduler>("mt"));
+    std::unique_ptr<RenderProcessScheduler> sched(
+        ComponentFactory::Create<RenderProcessScheduler>(d->sched_type ? d->sched_type : "mt"));
+    if (!sched) return -7;
     {
         HarnessNode* n = root.Add("scheduler");
         n->Add("num_samples", std::to_string(d->num_samples));

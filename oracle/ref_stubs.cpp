@@ -3,7 +3,8 @@
 // Link-time stand-ins for the parts of the reference runtime that its hot-path
 // sources call but that depend on libraries absent here (Boost.Regex,
 // pugixml, the logger thread):
-//   - Logger            (reference include/lightmetrica/logger.h:36-232): no-op sinks.
+//   - Logger            (reference include/lightmetrica/logger.h:36-232): no-op sinks
+//     except the last error, kept for lmref_last_error.
 //   - ComponentFactory  (reference include/lightmetrica/component.h:79-136): an
 //     in-process registry map; plugins are linked in, not dlopen'ed.
 //   - ConfigNode        (reference include/lightmetrica/confignode.h:37-194): backed
@@ -26,9 +27,15 @@
 LM_NAMESPACE_BEGIN
 
 // ---------------------------------------------------------------- Logger ----
+// Errors are kept (the last one, for lmref_last_error); other levels are dropped.
+static std::string& LastError()
+{
+	static thread_local std::string e;
+	return e;
+}
 void Logger::Reset() {}
 void Logger::Clear() {}
-void Logger::Error(const std::string&, const std::string&) {}
+void Logger::Error(const std::string& message, const std::string&) { LastError() = message; }
 void Logger::Warn(const std::string&, const std::string&) {}
 void Logger::Info(const std::string&, const std::string&) {}
 void Logger::Debug(const std::string&, const std::string&) {}
@@ -255,4 +262,11 @@ extern "C" const char* lmref_registered_components()
 	out.clear();
 	for (auto& kv : lightmetrica::Registry()) out += kv.first + "\n";
 	return out.c_str();
+}
+
+// The last message logged at error level by the calling thread (reference
+// components and plugins report their failures this way).
+extern "C" const char* lmref_last_error()
+{
+	return lightmetrica::LastError().c_str();
 }
