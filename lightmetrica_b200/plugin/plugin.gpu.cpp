@@ -516,17 +516,17 @@ public:
 public:
 
     // The reference renderers' keys (pathtrace.cpp:122-154); the sampler's
-    // rng_seed seeds the core's counter-based random numbers (a seed from
-    // the system when absent, like the reference's default).
+    // rng_seed seeds the core's counter-based random numbers. Absent or
+    // negative (the random sampler's default is -1, randomsampler.cpp:54-60)
+    // means a seed from the system, as the reference takes one from the clock.
     virtual bool Configure(const ConfigNode& node, const Assets& assets, const Scene& scene, const RenderProcessScheduler& sched) override
     {
         node.ChildValueOrDefault("rr_depth", 1, rrDepth);
         node.ChildValueOrDefault("max_path_vertices", -1, maxPathVertices);
+        long long s = -1;
         const auto samplerNode = node.Child("sampler");
-        if (!samplerNode.Empty() && !samplerNode.Child("rng_seed").Empty())
-            seed = static_cast<uint64_t>(samplerNode.Child("rng_seed").Value<long long>());
-        else
-            seed = static_cast<uint64_t>(std::random_device{}());
+        if (!samplerNode.Empty()) samplerNode.ChildValueOrDefault("rng_seed", -1LL, s);
+        seed = s >= 0 ? static_cast<uint64_t>(s) : static_cast<uint64_t>(std::random_device{}());
         return true;
     }
 
