@@ -570,6 +570,12 @@ public:
         p.seed = seed;
         p.num_samples = n;
         p.sample_offset = offset;
+        std::string why;
+        if (!scene.PrepareRender(why))       // Preprocess prepares it; a caller that skipped it gets it here
+        {
+            LM_LOG_ERROR("Renderer '" + Type() + "' cannot render this scene: " + why);
+            return false;
+        }
         rescaled.assign(static_cast<size_t>(scene.FilmWidth()) * scene.FilmHeight() * 3, 0.0f);
         LmgpuRenderStats stats;
         if (lmgpu_render(scene.RenderHandle(), &p, rescaled.data(), &stats) != LMGPU_OK)
