@@ -76,7 +76,22 @@ class RenderProcessScheduler:
         self.wave_paths = 0
         self.progress_image_interval = -1.0
         self.progress_images = []
+        self.termination_mode = "samples"
+        self.termination_time = 0.0
         self.last_stats = None
+
+    def set_termination_mode(self, mode: str, time: float = 0.0) -> None:
+        """RenderProcessScheduler::SetTerminationMode (sched.h:85): "samples"
+        renders num_samples; "time" renders passes of num_samples until
+        `time` seconds have passed (at least one pass; the reference checks
+        the clock after every block of samples, this after every pass) and
+        rescales by the samples processed (sched.mt.cpp:174-256)."""
+        if mode not in ("samples", "time"):
+            raise ValueError("termination mode must be 'samples' or 'time'")
+        if mode == "time" and not time > 0:
+            raise ValueError("time mode needs a positive time")
+        self.termination_mode = mode
+        self.termination_time = float(time)
 
     def configure(self, node: Optional[dict] = None, assets=None) -> bool:
         node = node or {}
@@ -94,8 +109,8 @@ class RenderProcessScheduler:
         cam = scene.main_camera()
         if cam is None or cam.film is None:
             raise RuntimeError("scene has no main camera / film")
-        if self.progress_image_interval > 0.0:
-            return self._render_with_progress(renderer, scene, cam)
+        if self.progress_image_interval > 0.0 or self.termination_mode == "time":
+            return self._render_chunked(renderer, scene, cam)
         film = np.zeros((cam.film.height, cam.film.width, 3), np.float32)
         p = renderer.params(self.num_samples, film_fp64=self.film_fp64, wave_paths=self.wave_paths)
         st = N.RenderStats()
@@ -106,26 +121,37 @@ class RenderProcessScheduler:
         return film
 
 
-    def _render_with_progress(self, renderer, scene, cam) -> np.ndarray:
-        """progress_image_interval > 0 (sched.mt.cpp:197-228): the budget is
-        rendered in chunks into one device film; whenever more than the
-        interval (seconds) has passed since the last image, the film so far
-        is rescaled by W*H / processed samples and saved as
-        progress.<renderer>/%010d(.hdr|.exr)."""
+    def _render_chunked(self, renderer, scene, cam) -> np.ndarray:
+        """Chunks of samples into one device film, for progress images and
+        the time termination mode. progress_image_interval > 0
+        (sched.mt.cpp:197-228): whenever more than the interval (seconds) has
+        passed since the last image, the film so far is rescaled by W*H /
+        processed samples and saved as progress.<renderer>/%010d(.hdr|.exr).
+        Time mode: passes of num_samples until the time is up."""
         import os
         import time
         import torch
         W, H = cam.film.width, cam.film.height
         dev_film = torch.zeros(W * H * 3, dtype=torch.float64 if self.film_fp64 else torch.float32, device="cuda")
         stream = torch.cuda.current_stream().cuda_stream
-        chunk = max(W * H, self.num_samples // 64)
+        timed = self.termination_mode == "time"
+        chunk = self.num_samples if timed else max(W * H, self.num_samples // 64)
+        if timed and self.progress_image_interval > 0.0:
+            chunk = max(1, min(chunk, max(W * H, self.num_samples // 64)))
         done, count = 0, 0
-        last = time.perf_counter()
+        start = last = time.perf_counter()
         out_dir = "progress." + renderer.type()
         self.progress_images = []
         totals = {"rays_traced": 0, "shadow_rays": 0, "paths": 0, "waves": 0, "max_bounces_run": 0, "device_ms": 0.0}
-        while done < self.num_samples:
-            n = min(chunk, self.num_samples - done)
+        while True:
+            if timed:
+                if done > 0 and done % self.num_samples == 0 and time.perf_counter() - start >= self.termination_time:
+                    break
+                n = min(chunk, self.num_samples - done % self.num_samples)
+            else:
+                if done >= self.num_samples:
+                    break
+                n = min(chunk, self.num_samples - done)
             p = renderer.params(n, sample_offset=done, film_fp64=self.film_fp64, wave_paths=self.wave_paths)
             st = N.RenderStats()
             N.check(N.lib().lmgpu_render_device(scene.handle, ctypes.byref(p), ctypes.c_void_p(dev_film.data_ptr()),
@@ -135,14 +161,16 @@ class RenderProcessScheduler:
             totals["max_bounces_run"] = max(totals["max_bounces_run"], st.max_bounces_run)
             done += n
             now = time.perf_counter()
-            if now - last > self.progress_image_interval and done < self.num_samples:
+            more = timed or done < self.num_samples
+            if self.progress_image_interval > 0.0 and now - last > self.progress_image_interval and more:
                 count += 1
                 img = (dev_film.double().cpu().numpy() * (W * H / done)).astype(np.float32).reshape(H, W, 3)
                 from .film_io import save_film
                 self.progress_images.append(save_film(img, os.path.join(out_dir, "%010d" % count),
                                                       cam.film.image_type))
                 last = now
-        film = (dev_film.double().cpu().numpy() * (W * H / self.num_samples)).astype(np.float32).reshape(H, W, 3)
+        film = (dev_film.double().cpu().numpy() * (W * H / done)).astype(np.float32).reshape(H, W, 3)
+        totals["processed_samples"] = done
         self.last_stats = totals
         cam.film.data = film
         return film

@@ -141,3 +141,29 @@ def test_mpi_scheduler_on_one_rank_matches_mt(cuda):
     mt.configure({"num_samples": n})
     np.testing.assert_allclose(got, mt.render(r, scene), rtol=1e-4, atol=1e-6)
     scene.close()
+
+
+def test_time_termination_mode(cuda):
+    """Time mode renders whole passes of num_samples until the time is up;
+    the film is the rescaled sum of all processed samples, so it equals a
+    samples-mode render of that many samples (same sample indices)."""
+    prims = scenes.cornell_box(64, 64)
+    n = 64 * 64 * 16
+    scene = create_scene("bvh")
+    scene.load(prims)
+    scene.configure({})
+    scene.build()
+    r = create_renderer("pt.mis")
+    r.configure({"rr_depth": 3, "max_path_vertices": 9, "sampler": {"rng_seed": 4}})
+    s = create_scheduler("mt")
+    s.configure({"num_samples": n})
+    s.set_termination_mode("time", 0.25)
+    timed = s.render(r, scene)
+    done = s.last_stats["processed_samples"]
+    assert done >= n and done % n == 0
+    s2 = create_scheduler("mt")
+    s2.configure({"num_samples": done})
+    want = s2.render(r, scene)
+    scene.close()
+    np.testing.assert_allclose(timed, want, rtol=1e-4, atol=1e-6)
+
