@@ -74,7 +74,23 @@ class MPIRenderProcessScheduler:
         self.num_samples = 1
         self.samples_per_task = 1000000
         self.film_fp64 = True
+        self.termination_mode = "samples"
+        self.termination_time = 0.0
         self.last_shard = None
+        self.processed_samples = 0
+
+    def set_termination_mode(self, mode: str, time: float = 0.0) -> None:
+        """SetTerminationMode (sched.mpi.cpp:64): "samples" renders
+        num_samples over the ranks; "time" renders rounds of num_samples (each
+        rank its shard of each round) until rank 0 has seen `time` seconds
+        pass (at least one round; the reference hands out tasks until then,
+        sched.mpi.cpp:146-186), and rescales by the samples processed."""
+        if mode not in ("samples", "time"):
+            raise ValueError("termination mode must be 'samples' or 'time'")
+        if mode == "time" and not time > 0:
+            raise ValueError("time mode needs a positive time")
+        self.termination_mode = mode
+        self.termination_time = float(time)
 
     def configure(self, node: Optional[dict] = None, assets=None) -> bool:
         node = node or {}
@@ -107,17 +123,35 @@ class MPIRenderProcessScheduler:
         Returns the rescaled film (H, W, 3) on rank 0 and None elsewhere.
         `render_shard(offset, count)` returns the shard's un-rescaled film as
         a torch tensor of W*H*3 values (default: this rank's GPU)."""
+        import time
+        import torch
         import torch.distributed as dist
         rank, world = rank_and_world(group)
         offset, count = shard(self.num_samples, rank, world)
         self.last_shard = (offset, count)
-        film = (render_shard or (lambda o, c: self._gpu_shard(renderer, scene, o, c)))(offset, count)
+        render_shard = render_shard or (lambda o, c: self._gpu_shard(renderer, scene, o, c))
+        film = render_shard(offset, count)
+        rounds = 1
+        if self.termination_mode == "time":
+            # Rank 0 decides after each round and every rank follows, so all
+            # ranks take the same collective steps.
+            start = time.perf_counter()
+            while True:
+                go = torch.tensor([1 if time.perf_counter() - start < self.termination_time else 0],
+                                  dtype=torch.int32, device=film.device)
+                if world > 1:
+                    dist.broadcast(go, src=0, group=group)
+                if not int(go.item()):
+                    break
+                film = film + render_shard(rounds * self.num_samples + offset, count)
+                rounds += 1
+        self.processed_samples = rounds * self.num_samples
         if world > 1:
             dist.reduce(film, dst=0, op=dist.ReduceOp.SUM, group=group)
         if rank != 0:
             return None
         cam = scene.main_camera()
         W, H = cam.film.width, cam.film.height
-        out = (film.double().cpu().numpy() * (W * H / self.num_samples)).astype(np.float32).reshape(H, W, 3)
+        out = (film.double().cpu().numpy() * (W * H / self.processed_samples)).astype(np.float32).reshape(H, W, 3)
         cam.film.data = out
         return out

@@ -58,7 +58,7 @@ class _CameraOnly:
         return self.prims.camera
 
 
-def _worker(rank, world, port, out_dir):
+def _worker(rank, world, port, out_dir, time_limit=0.0):
     import torch
     import torch.distributed as dist
     import oracle
@@ -68,6 +68,8 @@ def _worker(rank, world, port, out_dir):
         n = 16 * 16 * SPP
         sched = create_scheduler("mpi")
         sched.configure({"num_samples": n})
+        if time_limit > 0:
+            sched.set_termination_mode("time", time_limit)
 
         def render_shard(offset, count):
             return torch.from_numpy(oracle.oracle_render_range(prims, offset, offset + count, "pt.mis", RR, MAX_PV,
@@ -75,7 +77,8 @@ def _worker(rank, world, port, out_dir):
         film = sched.render(None, _CameraOnly(prims), render_shard=render_shard)
         job = max_over_ranks(float(rank + 1))
         np.save(os.path.join(out_dir, f"rank{rank}.npy"),
-                {"film": film, "shard": sched.last_shard, "job": job}, allow_pickle=True)
+                {"film": film, "shard": sched.last_shard, "job": job, "processed": sched.processed_samples},
+                allow_pickle=True)
     finally:
         dist.destroy_process_group()
 
@@ -102,3 +105,31 @@ def test_two_ranks_reduce_to_the_one_process_film(tmp_path):
                                 seed=SEED, threads=2)
     assert want.max() > 0
     np.testing.assert_allclose(r0["film"], want, rtol=1e-5, atol=1e-7)
+
+
+def test_two_ranks_time_mode(tmp_path):
+    """Time mode: rank 0 decides after each round of num_samples and both
+    ranks follow; the reduced film is the one-process render of every
+    processed sample."""
+    import torch.multiprocessing as mp
+    import oracle
+    world = 2
+    mp.start_processes(_worker, args=(world, _free_port(), str(tmp_path), 0.5), nprocs=world, join=True,
+                       start_method="spawn")
+    r0 = np.load(tmp_path / "rank0.npy", allow_pickle=True).item()
+    r1 = np.load(tmp_path / "rank1.npy", allow_pickle=True).item()
+    n = 16 * 16 * SPP
+    done = r0["processed"]
+    assert done == r1["processed"] and done >= n and done % n == 0
+    assert r1["film"] is None
+    want = oracle.oracle_render_range(scenes.cornell_box(16, 16), 0, done, "pt.mis", RR, MAX_PV, SEED)
+    np.testing.assert_allclose(r0["film"], want.reshape(16, 16, 3) * (16 * 16 / done), rtol=1e-5, atol=1e-7)
+
+
+def test_mpi_termination_mode_validation():
+    s = create_scheduler("mpi")
+    s.set_termination_mode("time", 2.0)
+    assert (s.termination_mode, s.termination_time) == ("time", 2.0)
+    with pytest.raises(ValueError):
+        s.set_termination_mode("time", -1)
+
