@@ -374,6 +374,7 @@ int launch_diff(LmgpuScene* sc, const LmgpuRenderParams* p, const LmgpuDiffParam
                 const float* dL, float* da, float* de, cudaStream_t st, LmgpuRenderStats* stats)
 {
     if (!sc || !p) return fail(LMGPU_ERR_INVALID, "null argument");
+    if (const int rc = check_scene_device(sc)) return rc;
     if (!sc->dev.cam.valid) return fail(LMGPU_ERR_INVALID, "scene has no camera");
     if (p->num_samples <= 0) return fail(LMGPU_ERR_INVALID, "num_samples must be positive");
     if (p->technique < LMGPU_RENDER_PT || p->technique > LMGPU_RENDER_PT_MIS) return fail(LMGPU_ERR_INVALID, "unknown technique");

@@ -518,6 +518,7 @@ int lmgpu_scene_info(const LmgpuScene* scene, LmgpuSceneInfo* info)
 int lmgpu_intersect(LmgpuScene* scene, const LmgpuRaysSoA* rays, int64_t n, LmgpuHitsSoA* hits, void* stream)
 {
     if (!scene || !rays || !hits || n < 0) return fail(LMGPU_ERR_INVALID, "null argument or negative count");
+    if (const int rc = check_scene_device(scene)) return rc;
     if (n > 0 && (!rays->ox || !rays->oy || !rays->oz || !rays->dx || !rays->dy || !rays->dz || !rays->tmin || !rays->tmax))
         return fail(LMGPU_ERR_INVALID, "null ray array");
     return launch_intersect(scene, soa_src(*rays), n, *hits, static_cast<cudaStream_t>(stream), nullptr);
@@ -526,6 +527,7 @@ int lmgpu_intersect(LmgpuScene* scene, const LmgpuRaysSoA* rays, int64_t n, Lmgp
 int lmgpu_occluded(LmgpuScene* scene, const LmgpuRaysSoA* rays, int64_t n, uint8_t* occluded, void* stream)
 {
     if (!scene || !rays || !occluded || n < 0) return fail(LMGPU_ERR_INVALID, "null argument or negative count");
+    if (const int rc = check_scene_device(scene)) return rc;
     if (n == 0) return LMGPU_OK;
     return launch_trace<true>(scene, ApiAnyIO{ soa_src(*rays), n, occluded }, n, static_cast<cudaStream_t>(stream));
 }
@@ -533,6 +535,7 @@ int lmgpu_occluded(LmgpuScene* scene, const LmgpuRaysSoA* rays, int64_t n, uint8
 int lmgpu_intersect_host(LmgpuScene* scene, const float* rays_aos, int64_t n, int32_t* tri_id, float* t, float* u, float* v)
 {
     if (!scene || (n > 0 && !rays_aos) || n < 0) return fail(LMGPU_ERR_INVALID, "null argument or negative count");
+    if (const int rc = check_scene_device(scene)) return rc;
     if (n == 0) return LMGPU_OK;
     // Chunked pipeline over HostPipeline::SLOTS streams: uploads, traversals
     // and downloads of neighbouring chunks overlap (full-duplex PCIe).
@@ -577,6 +580,7 @@ int lmgpu_intersect_counted(LmgpuScene* scene, const LmgpuRaysSoA* rays, int64_t
                             unsigned long long* counters_device, void* stream)
 {
     if (!scene || !rays || !hits || !counters_device || n < 0) return fail(LMGPU_ERR_INVALID, "null argument");
+    if (const int rc = check_scene_device(scene)) return rc;
     return launch_intersect(scene, soa_src(*rays), n, *hits, static_cast<cudaStream_t>(stream), counters_device);
 }
 

@@ -56,6 +56,18 @@ int render_device_preallocated(LmgpuScene* sc, const LmgpuRenderParams& p, void*
 // Reads and clears the device status word; maps it to an LMGPU status.
 int consume_status(LmgpuScene* s, cudaStream_t stream);
 
+// The calling thread's current device must be the one the scene was created
+// on: the scene's buffers live there, and kernels launched elsewhere would
+// read another GPU's memory.
+inline int check_scene_device(const LmgpuScene* s)
+{
+    int cur = 0;
+    const cudaError_t e = cudaGetDevice(&cur);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if (cur != s->device) return fail(LMGPU_ERR_INVALID, "scene used on another device than it was created on");
+    return LMGPU_OK;
+}
+
 }  // namespace lmgpu
 
 #define LMGPU_CUDA_TRY(expr)                                              \
