@@ -158,7 +158,11 @@ int lmgpu_intersect(LmgpuScene* scene, const LmgpuRaysSoA* rays, int64_t n,
 
 /* Same query from HOST buffers: rays AoS (8 floats per ray: o.xyz, d.xyz,
  * minT, maxT), outputs to host arrays (any may be NULL). Copies in, traces,
- * copies out, synchronises. */
+ * copies out, synchronises; 2^20-ray chunks on four streams overlap their
+ * uploads, traversals and downloads. Page-locked buffers (cudaMallocHost,
+ * cudaHostRegister) are copied directly; pageable ones, in batches of 2^16
+ * rays or more, through the scene's pinned staging (192 MB, allocated on
+ * first use) filled and drained by a pool of host threads. */
 int lmgpu_intersect_host(LmgpuScene* scene, const float* rays_aos, int64_t n,
                          int32_t* tri_id, float* t, float* u, float* v);
 
@@ -211,7 +215,11 @@ typedef struct {
 
 /* Renders `num_samples` samples and writes the rescaled film (W*H*3 floats,
  * row y = 0 first, reference HDRBitmapFilm layout) to a HOST buffer:
- * the whole RenderProcessScheduler::Render (sched.mt.cpp:93-266) in one call. */
+ * the whole RenderProcessScheduler::Render (sched.mt.cpp:93-266) in one call.
+ * Keeps a device film, its rescaled copy and a pinned host copy per device
+ * between calls (about 3 * W*H*3*4 bytes for a float film); calls on one
+ * device take turns. The calling thread's current device must be the scene's
+ * (true of every call that takes a scene). */
 int lmgpu_render(LmgpuScene* scene, const LmgpuRenderParams* params,
                  float* film_host, LmgpuRenderStats* stats);
 

@@ -18,6 +18,12 @@ struct HostPipeline {
     cudaStream_t stream[SLOTS] = {};
     float* rays[SLOTS] = {};
     float* hits[SLOTS] = {};
+    // Pinned staging for callers' pageable buffers (allocated on first use):
+    // a chunk of rays and a chunk of hits per slot, and the event that marks
+    // the slot's hits as copied back.
+    float* stage_rays[SLOTS] = {};
+    float* stage_hits[SLOTS] = {};
+    cudaEvent_t done[SLOTS] = {};
 };
 
 struct LmgpuScene {

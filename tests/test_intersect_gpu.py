@@ -219,3 +219,27 @@ def test_host_pipeline_matches_device_path(cuda):
                            torch.cuda.current_stream().cuda_stream)
         s.status(torch.cuda.current_stream().cuda_stream)
         np.testing.assert_array_equal(a["tri_id"], out.cpu().numpy())
+
+
+@pytest.mark.parametrize("pinned_in,pinned_out", [(True, False), (False, True), (True, True)])
+def test_host_pipeline_pinned_and_pageable_buffers(cuda, pinned_in, pinned_out):
+    """Page-locked caller buffers go straight to the copy engines; pageable
+    ones through the pipeline's pinned staging (rays in, hits out, or both).
+    Same hits either way."""
+    import ctypes
+    import torch
+    from lightmetrica_b200 import native
+    pos, faces = random_soup(1 << 16, seed=63, sigma=0.03)
+    rays = random_rays(5 * (1 << 20) + 777, seed=64)
+    n = rays.shape[0]
+    s = gpu_scene(pos, faces, "bvh")
+    want = s.intersect_host(rays)                  # pageable in and out
+    rin = torch.from_numpy(rays).pin_memory() if pinned_in else torch.from_numpy(rays.copy())
+    outs = [torch.empty(n, dtype=dt) for dt in (torch.int32, torch.float32, torch.float32, torch.float32)]
+    if pinned_out:
+        outs = [o.pin_memory() for o in outs]
+    native.check(native.lib().lmgpu_intersect_host(s.handle, rin.data_ptr(), n, *[o.data_ptr() for o in outs]))
+    np.testing.assert_array_equal(outs[0].numpy(), want["tri_id"])
+    for o, k in zip(outs[1:], ("t", "u", "v")):
+        np.testing.assert_array_equal(o.numpy(), want[k])
+
