@@ -171,7 +171,12 @@ __device__ __forceinline__ int sample_light_diff(const DeviceScene& s, const Dif
 }
 
 template <int TECH, int LAYOUT, int STACK, bool BACKWARD>
-__global__ void __launch_bounds__(128) k_diff(const DeviceScene s, const DiffConsts c, float* image, const float* dL,
+// 8 resident blocks per SM (64 registers, some spills): on the refined
+// Cornell box, forward / backward 22.2 / 33.1 ms against 24.9 / 36.2 ms at the
+// unconstrained 94-96 registers (5 blocks); 6, 10 and 12 blocks were slower
+// in total. The passes are latency-bound and gain more from resident warps
+// than they lose to spills.
+__global__ void __launch_bounds__(128, 8) k_diff(const DeviceScene s, const DiffConsts c, float* image, const float* dL,
                                               float* d_albedo, float* d_emission, int32_t* status)
 {
     int2 stack[STACK];
