@@ -44,10 +44,12 @@ constexpr int POOLS = 2;                   // path pools (overlap mode uses both
 constexpr int DEFAULT_OVERLAP_BOUNCE = 3;
 constexpr int GRAPH_BOUNCES_UNBOUNDED = 24;
 constexpr int MAX_BOUNDED_BOUNCES = 64;
-// path state + scene index + sample index, depth, free list, retire queue;
-// the shadow arrays hold 2 entries per path (in stream mode a new path's
-// camera-vertex shadow ray and its first bounce's share one shadow pass).
-constexpr size_t BYTES_PER_PATH = 16 * 10 + 16 * 3 + 8 + 4 * 2 + 4 + 8 + 4 + 4 + 4;
+// path state (two ray queues of 32-byte records, hits, throughput, radiance,
+// previous vertex, shadow rays, raster) + sample index, scene index, depth,
+// free list, retire queue; the shadow arrays hold 2 entries per path (in
+// stream mode a new path's camera-vertex shadow ray and its first bounce's
+// share one shadow pass).
+constexpr size_t BYTES_PER_PATH = 16 * 12 + 16 * 3 + 8 + 8 + 4 + 4 + 4 + 4;
 constexpr int STREAM_CHECK_EVERY = 8;      // graph launches between checks of the done flag
 
 // Device totals of a render: [0] closest-hit rays, [1] shadow rays,
@@ -246,7 +248,7 @@ struct Wave {
         const PathState& st = b->st[l];
         const int qin = (k - 1) & 1;
         k_bounce_prep<<<1, 1, 0, s>>>(st.counters, qin, k, b->d_stats);
-        PathRayIO<true> io{ st.queue[qin], st.counters + qin, st.ray_o, st.ray_d, st.hit, b->d_table, st.scene };
+        PathRayIO<true> io{ st.counters + qin, st.qo[qin], st.qd[qin], st.hit, b->d_table };
         k_trace_persistent<LAYOUT, STACK, false, PathRayIO<true>><<<L.trace_blocks, 128, 0, s>>>(
             L.proto, io, b->d_status, work(b, l) + slot);
         k_pt_shade<TECH, Ctx><<<L.shade_blocks, 128, 0, s>>>(ctx(b, l), st, k, qin, 1 - qin);
@@ -306,7 +308,7 @@ struct Stream {
         unsigned long long* work = b->d_work + 2 * q;
         k_stream_plan<<<1, 1, 0, s>>>(b->d_ctl, st.counters, q, b->d_stats, work);
         k_pt_init<TECH, Ctx><<<(unsigned)((L.paths + 127) / 128), 128, 0, s>>>(make<Ctx>(b), st, 0, q);
-        PathRayIO<true> io{ st.queue[q], st.counters + q, st.ray_o, st.ray_d, st.hit, b->d_table, st.scene };
+        PathRayIO<true> io{ st.counters + q, st.qo[q], st.qd[q], st.hit, b->d_table };
         k_trace_persistent<LAYOUT, STACK, false, PathRayIO<true>><<<L.trace_blocks, 128, 0, s>>>(
             L.proto, io, b->d_status, work);
         k_pt_shade<TECH, Ctx><<<L.shade_blocks, 128, 0, s>>>(make<Ctx>(b), st, 0, q, 1 - q);
@@ -362,8 +364,10 @@ int ensure_batch_workspace(LmgpuBatch* b, int64_t paths, int pools)
         auto take = [&](size_t n) { char* r = p; p += n; return r; };
         PathState& st = b->st[l];
         st.counters = reinterpret_cast<uint32_t*>(take(256));
-        st.ray_o = reinterpret_cast<float4*>(take(16 * P));
-        st.ray_d = reinterpret_cast<float4*>(take(16 * P));
+        for (int q = 0; q < 2; q++) {
+            st.qo[q] = reinterpret_cast<float4*>(take(16 * P));
+            st.qd[q] = reinterpret_cast<float4*>(take(16 * P));
+        }
         st.hit = reinterpret_cast<float4*>(take(16 * P));
         st.thr = reinterpret_cast<float4*>(take(16 * P));
         st.L = reinterpret_cast<float4*>(take(16 * P));
@@ -374,8 +378,6 @@ int ensure_batch_workspace(LmgpuBatch* b, int64_t paths, int pools)
         st.sh_c = reinterpret_cast<float4*>(take(2 * 16 * P));
         st.sample = reinterpret_cast<int64_t*>(take(8 * P));      // 8-byte arrays first: alignment
         st.raster = reinterpret_cast<float2*>(take(8 * P));
-        st.queue[0] = reinterpret_cast<int32_t*>(take(4 * P));
-        st.queue[1] = reinterpret_cast<int32_t*>(take(4 * P));
         st.scene = reinterpret_cast<int32_t*>(take(4 * P));
         st.depth = reinterpret_cast<int32_t*>(take(4 * P));
         st.free_slots = reinterpret_cast<int32_t*>(take(4 * P));

@@ -99,7 +99,7 @@ void launch_full(const LmgpuScene* sc, const float* rays, int64_t n, int32_t* id
 // ------------------------------------------------------------ driver ------
 
 // Wave workspace (scratch), one per device, grown on demand.
-// Default paths per wave (32M: 5.9 GB of path state). Each bounce launch
+// Default paths per wave (32M: 6.7 GB of path state). Each bounce launch
 // ends with a latency-bound tail of the wave's longest rays, so fewer,
 // larger waves keep the GPU busier: on the 1080p terrain, waves of 4M, 8M,
 // 16M and 32M paths gave 0.94, 1.20, 1.40 and 1.53 Grays/s.
@@ -113,22 +113,22 @@ struct Workspace {
     PathState st{};
 };
 
-int ensure_workspace(Workspace& ws, int64_t paths)
+// Path state bytes per path (two ray queues of 32-byte records, hits,
+// throughput, radiance, previous vertex, shadow rays, raster) and the fixed
+// header of counters.
+constexpr size_t WS_BYTES_PER_PATH = 16 * 12 + 8;
+constexpr size_t WS_HEADER_BYTES = 256;
+
+// Lays the path state of P paths out from `p` (WS_HEADER_BYTES +
+// P * WS_BYTES_PER_PATH bytes, 256-byte aligned).
+void carve_state(PathState& st, char* p, size_t P)
 {
-    if (!ws.host_counts) LMGPU_CUDA_TRY(cudaMallocHost(&ws.host_counts, 16));
-    if (ws.capacity >= paths && ws.mem) return LMGPU_OK;
-    if (ws.mem) { cudaFree(ws.mem); ws.mem = nullptr; ws.capacity = 0; }
-    const size_t P = (size_t)paths;
-    const size_t bytes = P * (16 * 10 + 8 + 4 * 2) + 256;
-    cudaError_t e = cudaMalloc(&ws.mem, bytes);
-    if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? fail(LMGPU_ERR_OOM, "render workspace allocation failed")
-                                                                 : cuda_fail(e, "cudaMalloc(workspace)");
-    char* p = static_cast<char*>(ws.mem);
     auto take = [&](size_t b) { char* r = p; p += b; return r; };
-    PathState& st = ws.st;
-    st.counters = reinterpret_cast<uint32_t*>(take(256));
-    st.ray_o = reinterpret_cast<float4*>(take(16 * P));
-    st.ray_d = reinterpret_cast<float4*>(take(16 * P));
+    st.counters = reinterpret_cast<uint32_t*>(take(WS_HEADER_BYTES));
+    for (int q = 0; q < 2; q++) {
+        st.qo[q] = reinterpret_cast<float4*>(take(16 * P));
+        st.qd[q] = reinterpret_cast<float4*>(take(16 * P));
+    }
     st.hit = reinterpret_cast<float4*>(take(16 * P));
     st.thr = reinterpret_cast<float4*>(take(16 * P));
     st.L = reinterpret_cast<float4*>(take(16 * P));
@@ -138,8 +138,18 @@ int ensure_workspace(Workspace& ws, int64_t paths)
     st.sh_d = reinterpret_cast<float4*>(take(16 * P));
     st.sh_c = reinterpret_cast<float4*>(take(16 * P));
     st.raster = reinterpret_cast<float2*>(take(8 * P));
-    st.queue[0] = reinterpret_cast<int32_t*>(take(4 * P));
-    st.queue[1] = reinterpret_cast<int32_t*>(take(4 * P));
+}
+
+int ensure_workspace(Workspace& ws, int64_t paths)
+{
+    if (!ws.host_counts) LMGPU_CUDA_TRY(cudaMallocHost(&ws.host_counts, 16));
+    if (ws.capacity >= paths && ws.mem) return LMGPU_OK;
+    if (ws.mem) { cudaFree(ws.mem); ws.mem = nullptr; ws.capacity = 0; }
+    const size_t P = (size_t)paths;
+    cudaError_t e = cudaMalloc(&ws.mem, WS_HEADER_BYTES + P * WS_BYTES_PER_PATH);
+    if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? fail(LMGPU_ERR_OOM, "render workspace allocation failed")
+                                                                 : cuda_fail(e, "cudaMalloc(workspace)");
+    carve_state(ws.st, static_cast<char*>(ws.mem), P);
     ws.capacity = paths;
     return LMGPU_OK;
 }
@@ -205,7 +215,7 @@ int render_waves(LmgpuScene* sc, const LmgpuRenderParams& p, F* film, cudaStream
             if (n == 0) break;
             stats.rays_traced += n;
             stats.max_bounces_run = std::max(stats.max_bounces_run, k);
-            PathRayIO<false> io{ st.queue[qin], st.counters + qin, st.ray_o, st.ray_d, st.hit, nullptr, nullptr };
+            PathRayIO<false> io{ st.counters + qin, st.qo[qin], st.qd[qin], st.hit, nullptr };
             rc = launch_trace<false>(sc, io, n, stream);
             if (rc != LMGPU_OK) break;
             LMGPU_CUDA_TRY(cudaMemsetAsync(st.counters + (1 - qin), 0, 4, stream));
@@ -337,33 +347,13 @@ int ensure_host_film(HostFilmBuffers& hb, size_t film_bytes, size_t out_bytes)
 }
 
 // Bytes of wave workspace per path (ensure_workspace's layout) and the
-// fixed header of counters.
-constexpr size_t WS_BYTES_PER_PATH = 16 * 10 + 8 + 4 * 2;
-constexpr size_t WS_HEADER_BYTES = 256;
 
 // Points a Workspace at caller-owned memory (same layout as
 // ensure_workspace, no allocation); host_counts is the caller's readback
 // buffer for the queue counters.
 void carve_workspace(Workspace& ws, void* mem, int64_t paths, uint32_t* host_counts)
 {
-    const size_t P = (size_t)paths;
-    char* p = static_cast<char*>(mem);
-    auto take = [&](size_t b) { char* r = p; p += b; return r; };
-    PathState& st = ws.st;
-    st.counters = reinterpret_cast<uint32_t*>(take(WS_HEADER_BYTES));
-    st.ray_o = reinterpret_cast<float4*>(take(16 * P));
-    st.ray_d = reinterpret_cast<float4*>(take(16 * P));
-    st.hit = reinterpret_cast<float4*>(take(16 * P));
-    st.thr = reinterpret_cast<float4*>(take(16 * P));
-    st.L = reinterpret_cast<float4*>(take(16 * P));
-    st.prev_p = reinterpret_cast<float4*>(take(16 * P));
-    st.prev_n = reinterpret_cast<float4*>(take(16 * P));
-    st.sh_o = reinterpret_cast<float4*>(take(16 * P));
-    st.sh_d = reinterpret_cast<float4*>(take(16 * P));
-    st.sh_c = reinterpret_cast<float4*>(take(16 * P));
-    st.raster = reinterpret_cast<float2*>(take(8 * P));
-    st.queue[0] = reinterpret_cast<int32_t*>(take(4 * P));
-    st.queue[1] = reinterpret_cast<int32_t*>(take(4 * P));
+    carve_state(ws.st, static_cast<char*>(mem), (size_t)paths);
     ws.mem = mem;
     ws.capacity = paths;
     ws.host_counts = host_counts;

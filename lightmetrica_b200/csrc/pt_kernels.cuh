@@ -40,17 +40,18 @@ namespace lmgpu {
 constexpr uint32_t PREV_DEGENERATED = 1u;   // previous vertex is the pinhole
 constexpr uint32_t PREV_SPECULAR = 2u;      // last BSDF sample was specular
 
-// Device pointers of one wave's path state (capacity paths).
+// Device pointers of one wave's path state (capacity paths). The two ray
+// queues hold the rays themselves in queue order (see queue_ray), so the
+// traversal and the shading read them, and the hits, contiguously.
 struct PathState {
-    float4* ray_o;     // o.xyz, minT
-    float4* ray_d;     // d.xyz
-    float4* hit;       // tri (int bits), t, u, v
+    float4* qo[2];     // queued ray: origin, scene index (int bits)
+    float4* qd[2];     // direction, path slot | QUEUE_TMIN_ZERO (uint bits)
+    float4* hit;       // by slot of the traced queue: tri (int bits), t, u, v
     float4* thr;       // throughput
     float4* L;         // radiance to splat at the path's raster position
     float2* raster;
     float4* prev_p;    // previous vertex position, BSDF pdf (projected solid angle)
     float4* prev_n;    // previous vertex shading normal, flags (uint bits)
-    int32_t* queue[2];
     float4* sh_o;      // shadow ray origin, maxT
     float4* sh_d;      // direction, target (int bits: path index, or ~pixel)
     float4* sh_c;      // contribution, scene index (int bits)
@@ -230,6 +231,24 @@ __device__ __forceinline__ uint32_t queue_append(uint32_t* counter, bool want)
 __device__ __forceinline__ V3 f3(float4 q) { return v3(q.x, q.y, q.z); }
 __device__ __forceinline__ float4 f4(V3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
 
+// A queued ray's minT is Eps, except pt's camera rays (minT 0,
+// pathtrace.cpp:187, 245); the flag shares the word of the path slot
+// (slots < 2^31).
+constexpr uint32_t QUEUE_TMIN_ZERO = 0x80000000u;
+
+__device__ __forceinline__ void queue_ray(const PathState& st, int q, uint32_t slot, V3 o, V3 d, int64_t i, int sid,
+                                          bool tmin_zero)
+{
+    st.qo[q][slot] = f4(o, __int_as_float(sid));
+    st.qd[q][slot] = f4(d, __uint_as_float((uint32_t)i | (tmin_zero ? QUEUE_TMIN_ZERO : 0u)));
+}
+__device__ __forceinline__ int32_t queued_path(float4 d) { return (int32_t)(__float_as_uint(d.w) & ~QUEUE_TMIN_ZERO); }
+__device__ __forceinline__ float queued_tmin(float4 d)
+{
+    return (__float_as_uint(d.w) & QUEUE_TMIN_ZERO) ? 0.0f : EPS_F;
+}
+__device__ __forceinline__ int queued_scene(float4 o) { return __float_as_int(o.w); }
+
 template <class F>
 __device__ __forceinline__ void film_add(F* film, int pixel, V3 c)
 {
@@ -328,11 +347,7 @@ __global__ void __launch_bounds__(128) k_pt_init(const Ctx ctx, const PathState 
     }
     st.thr[i] = f4(thr, 0.0f);
     const uint32_t slot = queue_append(&st.counters[q], alive);
-    if (alive) {
-        st.ray_o[i] = f4(cp, TECH == LMGPU_RENDER_PT ? 0.0f : EPS_F);
-        st.ray_d[i] = f4(dir, 0.0f);
-        st.queue[q][slot] = (int32_t)i;
-    }
+    if (alive) queue_ray(st, q, slot, cp, dir, i, sid, TECH == LMGPU_RENDER_PT);
     if (Ctx::STREAM) {                           // a path that ends at the camera retires at once
         const uint32_t r = queue_append(&st.counters[3], !alive);
         if (!alive) st.retire[r] = (int32_t)i;
@@ -357,28 +372,25 @@ struct PathRayIO {
     static constexpr bool PER_RAY_SCENE = TABLE;
     static constexpr int REFILL_MIN = PATH_QUEUE_REFILL_MIN;
     static constexpr int EXIT_BELOW = PATH_QUEUE_EXIT_BELOW;
-    const int32_t* queue;
     const uint32_t* count_ptr;
-    const float4* ray_o;
-    const float4* ray_d;
+    const float4* qo;
+    const float4* qd;
     float4* hit;
     const BatchEntry* table;      // TABLE only
-    const int32_t* path_scene;    // TABLE only
     __device__ int64_t count() const { return (int64_t)*count_ptr; }
-    __device__ const DeviceScene& ray_scene(int64_t j) const { return table[path_scene[queue[j]]].s; }
+    __device__ const DeviceScene& ray_scene(int64_t j) const { return table[queued_scene(qo[j])].s; }
     __device__ RayIn load(int64_t j) const
     {
-        const int32_t i = queue[j];
-        const float4 o = ray_o[i], d = ray_d[i];
+        const float4 o = qo[j], d = qd[j];
         RayIn r;
         r.o[0] = o.x; r.o[1] = o.y; r.o[2] = o.z;
         r.d[0] = d.x; r.d[1] = d.y; r.d[2] = d.z;
-        r.tmin = o.w; r.tmax = FLT_MAX;
+        r.tmin = queued_tmin(d); r.tmax = FLT_MAX;
         return r;
     }
     __device__ void store(int64_t j, const Hit& h, const TraversalRay&) const
     {
-        hit[queue[j]] = make_float4(__int_as_float(h.tri), h.t, h.u, h.v);
+        hit[j] = make_float4(__int_as_float(h.tri), h.t, h.u, h.v);
     }
 };
 
@@ -445,8 +457,10 @@ __global__ void __launch_bounds__(128, LMGPU_PT_SHADE_MIN_BLOCKS) k_pt_shade(con
     for (int64_t r = 0; r < rounds; r++) {
         const int64_t j = r * stride + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
         const bool valid = j < count;
-        const int32_t i = valid ? st.queue[qin][j] : 0;
-        const int sid = valid ? ctx.path_scene(st, i) : 0;
+        const float4 o4 = valid ? st.qo[qin][j] : make_float4(0, 0, 0, 0);
+        const float4 d4 = valid ? st.qd[qin][j] : make_float4(0, 0, 0, 0);
+        const int32_t i = queued_path(d4);
+        const int sid = queued_scene(o4);
         const int k = valid ? ctx.path_depth(st, i, kw) : kw;   // this bounce's index
         bool alive = false, shadow = false;
         V3 thr = v3(0, 0, 0), L = v3(0, 0, 0);
@@ -457,8 +471,7 @@ __global__ void __launch_bounds__(128, LMGPU_PT_SHADE_MIN_BLOCKS) k_pt_shade(con
             const DeviceScene& s = ctx.scene(sid);
             const RenderConsts& rc = ctx.consts(sid);
             const uint64_t key = sample_key(rc.seed, (uint64_t)ctx.sample_of(sid, i));
-            const float4 h4 = st.hit[i];
-            const float4 o4 = st.ray_o[i], d4 = st.ray_d[i];
+            const float4 h4 = st.hit[j];
             const V3 ro = f3(o4), rd = f3(d4);
             const V3 wi = -rd;
             thr = f3(st.thr[i]);
@@ -472,7 +485,7 @@ __global__ void __launch_bounds__(128, LMGPU_PT_SHADE_MIN_BLOCKS) k_pt_shade(con
             m.R = v3(0, 0, 0);
             if (tri < 0) {
                 float t;
-                if (s.has_env && env_sphere_intersect(s, ro, rd, o4.w, FLT_MAX, t)) {
+                if (s.has_env && env_sphere_intersect(s, ro, rd, queued_tmin(d4), FLT_MAX, t)) {
                     env_surface(s, ro, rd, t, g);
                     Le = emitted(load3(s.env_Le), g.sn, wi);
                     light_pdf_area = s.env_inv_area;
@@ -556,13 +569,11 @@ __global__ void __launch_bounds__(128, LMGPU_PT_SHADE_MIN_BLOCKS) k_pt_shade(con
         const uint32_t slot = queue_append(&st.counters[qout], alive);
         if (alive) {
             st.thr[i] = f4(thr, 0.0f);
-            st.ray_o[i] = f4(g.p, EPS_F);
-            st.ray_d[i] = f4(bs.wo, 0.0f);
+            queue_ray(st, qout, slot, g.p, bs.wo, i, sid, false);
             if (TECH != LMGPU_RENDER_PT) {
                 st.prev_p[i] = f4(g.p, bs.pdf);
                 st.prev_n[i] = f4(g.sn, __uint_as_float(bs.specular ? PREV_SPECULAR : 0u));
             }
-            st.queue[qout][slot] = i;
             if (Ctx::STREAM) st.depth[i] = k + 1;
         }
         if constexpr (Ctx::STREAM) {
