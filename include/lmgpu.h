@@ -228,7 +228,7 @@ int lmgpu_render(LmgpuScene* scene, const LmgpuRenderParams* params,
  * W*H/num_samples. The call returns once the render's device work is done
  * (it reads each bounce's queue sizes back to size the next launch). Waves
  * hold `wave_paths` paths (0 = 2^25, fewer if device memory is short) in a
- * workspace of about 200 bytes per path that is shared by all scenes of the
+ * workspace of about 216 bytes per path that is shared by all scenes of the
  * device and kept until exit; calls on one device take turns. */
 int lmgpu_render_device(LmgpuScene* scene, const LmgpuRenderParams* params,
                         void* film_device, void* stream, LmgpuRenderStats* stats);

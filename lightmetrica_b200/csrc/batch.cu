@@ -44,12 +44,11 @@ constexpr int POOLS = 2;                   // path pools (overlap mode uses both
 constexpr int DEFAULT_OVERLAP_BOUNCE = 3;
 constexpr int GRAPH_BOUNCES_UNBOUNDED = 24;
 constexpr int MAX_BOUNDED_BOUNCES = 64;
-// path state (two ray queues of 32-byte records, hits, throughput, radiance,
-// previous vertex, shadow rays, raster) + sample index, scene index, depth,
-// free list, retire queue; the shadow arrays hold 2 entries per path (in
-// stream mode a new path's camera-vertex shadow ray and its first bounce's
-// share one shadow pass).
-constexpr size_t BYTES_PER_PATH = 16 * 12 + 16 * 3 + 8 + 8 + 4 + 4 + 4 + 4;
+// path state (two queues of 64-byte ray records, hits, radiance, shadow
+// rays, raster) + sample index, scene index, depth, free list, retire queue;
+// the shadow arrays hold 2 entries per path (in stream mode a new path's
+// camera-vertex shadow ray and its first bounce's share one shadow pass).
+constexpr size_t BYTES_PER_PATH = 16 * 13 + 16 * 3 + 8 + 8 + 4 + 4 + 4 + 4;
 constexpr int STREAM_CHECK_EVERY = 8;      // graph launches between checks of the done flag
 
 // Device totals of a render: [0] closest-hit rays, [1] shadow rays,
@@ -367,12 +366,11 @@ int ensure_batch_workspace(LmgpuBatch* b, int64_t paths, int pools)
         for (int q = 0; q < 2; q++) {
             st.qo[q] = reinterpret_cast<float4*>(take(16 * P));
             st.qd[q] = reinterpret_cast<float4*>(take(16 * P));
+            st.qt[q] = reinterpret_cast<float4*>(take(16 * P));
+            st.qn[q] = reinterpret_cast<float4*>(take(16 * P));
         }
         st.hit = reinterpret_cast<float4*>(take(16 * P));
-        st.thr = reinterpret_cast<float4*>(take(16 * P));
         st.L = reinterpret_cast<float4*>(take(16 * P));
-        st.prev_p = reinterpret_cast<float4*>(take(16 * P));
-        st.prev_n = reinterpret_cast<float4*>(take(16 * P));
         st.sh_o = reinterpret_cast<float4*>(take(2 * 16 * P));
         st.sh_d = reinterpret_cast<float4*>(take(2 * 16 * P));
         st.sh_c = reinterpret_cast<float4*>(take(2 * 16 * P));

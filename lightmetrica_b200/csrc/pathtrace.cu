@@ -99,7 +99,7 @@ void launch_full(const LmgpuScene* sc, const float* rays, int64_t n, int32_t* id
 // ------------------------------------------------------------ driver ------
 
 // Wave workspace (scratch), one per device, grown on demand.
-// Default paths per wave (32M: 6.7 GB of path state). Each bounce launch
+// Default paths per wave (32M: 7.2 GB of path state). Each bounce launch
 // ends with a latency-bound tail of the wave's longest rays, so fewer,
 // larger waves keep the GPU busier: on the 1080p terrain, waves of 4M, 8M,
 // 16M and 32M paths gave 0.94, 1.20, 1.40 and 1.53 Grays/s.
@@ -113,10 +113,9 @@ struct Workspace {
     PathState st{};
 };
 
-// Path state bytes per path (two ray queues of 32-byte records, hits,
-// throughput, radiance, previous vertex, shadow rays, raster) and the fixed
-// header of counters.
-constexpr size_t WS_BYTES_PER_PATH = 16 * 12 + 8;
+// Path state bytes per path (two queues of 64-byte ray records, hits,
+// radiance, shadow rays, raster) and the fixed header of counters.
+constexpr size_t WS_BYTES_PER_PATH = 16 * 13 + 8;
 constexpr size_t WS_HEADER_BYTES = 256;
 
 // Lays the path state of P paths out from `p` (WS_HEADER_BYTES +
@@ -128,12 +127,11 @@ void carve_state(PathState& st, char* p, size_t P)
     for (int q = 0; q < 2; q++) {
         st.qo[q] = reinterpret_cast<float4*>(take(16 * P));
         st.qd[q] = reinterpret_cast<float4*>(take(16 * P));
+        st.qt[q] = reinterpret_cast<float4*>(take(16 * P));
+        st.qn[q] = reinterpret_cast<float4*>(take(16 * P));
     }
     st.hit = reinterpret_cast<float4*>(take(16 * P));
-    st.thr = reinterpret_cast<float4*>(take(16 * P));
     st.L = reinterpret_cast<float4*>(take(16 * P));
-    st.prev_p = reinterpret_cast<float4*>(take(16 * P));
-    st.prev_n = reinterpret_cast<float4*>(take(16 * P));
     st.sh_o = reinterpret_cast<float4*>(take(16 * P));
     st.sh_d = reinterpret_cast<float4*>(take(16 * P));
     st.sh_c = reinterpret_cast<float4*>(take(16 * P));

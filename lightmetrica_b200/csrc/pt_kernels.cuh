@@ -41,17 +41,17 @@ constexpr uint32_t PREV_DEGENERATED = 1u;   // previous vertex is the pinhole
 constexpr uint32_t PREV_SPECULAR = 2u;      // last BSDF sample was specular
 
 // Device pointers of one wave's path state (capacity paths). The two ray
-// queues hold the rays themselves in queue order (see queue_ray), so the
-// traversal and the shading read them, and the hits, contiguously.
+// queues hold each live path's ray and its state between bounces in queue
+// order (see queue_ray), so the traversal and the shading read them, and
+// the hits, contiguously; the ray's origin is the previous vertex.
 struct PathState {
     float4* qo[2];     // queued ray: origin, scene index (int bits)
     float4* qd[2];     // direction, path slot | QUEUE_TMIN_ZERO (uint bits)
+    float4* qt[2];     // throughput, previous vertex's BSDF pdf (projected solid angle)
+    float4* qn[2];     // previous vertex's shading normal, flags (uint bits); pt.direct / pt.mis
     float4* hit;       // by slot of the traced queue: tri (int bits), t, u, v
-    float4* thr;       // throughput
     float4* L;         // radiance to splat at the path's raster position
     float2* raster;
-    float4* prev_p;    // previous vertex position, BSDF pdf (projected solid angle)
-    float4* prev_n;    // previous vertex shading normal, flags (uint bits)
     float4* sh_o;      // shadow ray origin, maxT
     float4* sh_d;      // direction, target (int bits: path index, or ~pixel)
     float4* sh_c;      // contribution, scene index (int bits)
@@ -236,11 +236,14 @@ __device__ __forceinline__ float4 f4(V3 v, float w) { return make_float4(v.x, v.
 // (slots < 2^31).
 constexpr uint32_t QUEUE_TMIN_ZERO = 0x80000000u;
 
+template <int TECH>
 __device__ __forceinline__ void queue_ray(const PathState& st, int q, uint32_t slot, V3 o, V3 d, int64_t i, int sid,
-                                          bool tmin_zero)
+                                          bool tmin_zero, V3 thr, float pdf, V3 n, uint32_t flags)
 {
     st.qo[q][slot] = f4(o, __int_as_float(sid));
     st.qd[q][slot] = f4(d, __uint_as_float((uint32_t)i | (tmin_zero ? QUEUE_TMIN_ZERO : 0u)));
+    st.qt[q][slot] = f4(thr, pdf);
+    if (TECH != LMGPU_RENDER_PT) st.qn[q][slot] = f4(n, __uint_as_float(flags));
 }
 __device__ __forceinline__ int32_t queued_path(float4 d) { return (int32_t)(__float_as_uint(d.w) & ~QUEUE_TMIN_ZERO); }
 __device__ __forceinline__ float queued_tmin(float4 d)
@@ -342,12 +345,9 @@ __global__ void __launch_bounds__(128) k_pt_init(const Ctx ctx, const PathState 
             if (rng_uniform(key, dim_vertex(1) + DIM_RR) > p) alive = false;
             else thr = thr / p;
         }
-        st.prev_p[i] = f4(cp, pdf_cam);
-        st.prev_n[i] = make_float4(0, 0, 1, __uint_as_float(PREV_DEGENERATED));
     }
-    st.thr[i] = f4(thr, 0.0f);
     const uint32_t slot = queue_append(&st.counters[q], alive);
-    if (alive) queue_ray(st, q, slot, cp, dir, i, sid, TECH == LMGPU_RENDER_PT);
+    if (alive) queue_ray<TECH>(st, q, slot, cp, dir, i, sid, TECH == LMGPU_RENDER_PT, thr, pdf_cam, v3(0, 0, 1), PREV_DEGENERATED);
     if (Ctx::STREAM) {                           // a path that ends at the camera retires at once
         const uint32_t r = queue_append(&st.counters[3], !alive);
         if (!alive) st.retire[r] = (int32_t)i;
@@ -463,7 +463,7 @@ __global__ void __launch_bounds__(128, LMGPU_PT_SHADE_MIN_BLOCKS) k_pt_shade(con
         const int sid = queued_scene(o4);
         const int k = valid ? ctx.path_depth(st, i, kw) : kw;   // this bounce's index
         bool alive = false, shadow = false;
-        V3 thr = v3(0, 0, 0), L = v3(0, 0, 0);
+        V3 thr = v3(0, 0, 0);
         Geom g;
         BsdfSample bs;
         V3 sh_target = v3(0, 0, 0), sh_c = v3(0, 0, 0);
@@ -474,8 +474,8 @@ __global__ void __launch_bounds__(128, LMGPU_PT_SHADE_MIN_BLOCKS) k_pt_shade(con
             const float4 h4 = st.hit[j];
             const V3 ro = f3(o4), rd = f3(d4);
             const V3 wi = -rd;
-            thr = f3(st.thr[i]);
-            L = f3(st.L[i]);
+            const float4 t4 = st.qt[qin][j];
+            thr = f3(t4);
             const int32_t tri = __float_as_int(h4.x);
             V3 Le = v3(0, 0, 0);
             float light_pdf_area = 0.0f;   // EvaluatePositionPDF of the light that was hit
@@ -502,20 +502,26 @@ __global__ void __launch_bounds__(128, LMGPU_PT_SHADE_MIN_BLOCKS) k_pt_shade(con
                 m = material_of(s, prim);
                 hit_surface = true;
             }
-            // ---- emission reached by BSDF sampling
+            // ---- emission reached by BSDF sampling (the path's radiance is
+            // read and written only here; shadow rays add to it later)
             if (!is_zero(Le)) {
-                if (TECH == LMGPU_RENDER_PT) {
-                    L = L + thr * Le;
-                } else {
-                    const float4 pp = st.prev_p[i], pn = st.prev_n[i];
+                bool add = true;
+                V3 c = thr * Le;
+                if (TECH != LMGPU_RENDER_PT) {
+                    const float4 pn = st.qn[qin][j];   // previous vertex: position ro, pdf t4.w
                     const uint32_t flags = __float_as_uint(pn.w);
                     if (flags & PREV_SPECULAR) {
-                        L = L + thr * Le;
                     } else if (TECH == LMGPU_RENDER_PT_MIS) {
-                        const float G = geometry_term(f3(pp), f3(pn), (flags & PREV_DEGENERATED) != 0, g.p, g.sn, false);
+                        const float G = geometry_term(ro, f3(pn), (flags & PREV_DEGENERATED) != 0, g.p, g.sn, false);
                         const float pdf_dl = G == 0.0f ? 0.0f : light_pdf_area / (float(s.num_lights) * G);
-                        L = L + thr * Le * (pp.w / (pp.w + pdf_dl));
+                        c = thr * Le * (t4.w / (t4.w + pdf_dl));
+                    } else {
+                        add = false;
                     }
+                }
+                if (add) {
+                    const V3 L = f3(st.L[i]) + c;
+                    st.L[i] = f4(L, 0.0f);
                 }
             }
             const int v = k + 1;   // numPathVertices once this hit is accepted
@@ -562,18 +568,12 @@ __global__ void __launch_bounds__(128, LMGPU_PT_SHADE_MIN_BLOCKS) k_pt_shade(con
                 }
                 if (alive && TECH == LMGPU_RENDER_PT && rc.max_pv != -1 && k + 1 >= rc.max_pv) alive = false;
             }
-            st.L[i] = f4(L, 0.0f);
         }
         const uint32_t sslot = queue_append(&st.counters[2], shadow);
         if (shadow) write_shadow(st, sslot, g.p, sh_target, sh_c, i, sid);
         const uint32_t slot = queue_append(&st.counters[qout], alive);
         if (alive) {
-            st.thr[i] = f4(thr, 0.0f);
-            queue_ray(st, qout, slot, g.p, bs.wo, i, sid, false);
-            if (TECH != LMGPU_RENDER_PT) {
-                st.prev_p[i] = f4(g.p, bs.pdf);
-                st.prev_n[i] = f4(g.sn, __uint_as_float(bs.specular ? PREV_SPECULAR : 0u));
-            }
+            queue_ray<TECH>(st, qout, slot, g.p, bs.wo, i, sid, false, thr, bs.pdf, g.sn, bs.specular ? PREV_SPECULAR : 0u);
             if (Ctx::STREAM) st.depth[i] = k + 1;
         }
         if constexpr (Ctx::STREAM) {
