@@ -227,7 +227,7 @@ int lmgpu_render(LmgpuScene* scene, const LmgpuRenderParams* params,
  * (float, or double when film_fp64) on `stream`; the caller rescales by
  * W*H/num_samples. The call returns once the render's device work is done
  * (it reads each bounce's queue sizes back to size the next launch). Waves
- * hold `wave_paths` paths (0 = 2^25, fewer if device memory is short) in a
+ * hold `wave_paths` paths (0 = 2^27, fewer if device memory is short) in a
  * workspace of about 216 bytes per path that is shared by all scenes of the
  * device and kept until exit; calls on one device take turns. */
 int lmgpu_render_device(LmgpuScene* scene, const LmgpuRenderParams* params,
@@ -305,7 +305,7 @@ enum {
 typedef struct LmgpuBatchConfig {
     int32_t layout;               /* LMGPU_LAYOUT_BVH2 or LMGPU_LAYOUT_BVH4 for every scene */
     int32_t wave_paths;           /* paths in flight: the capacity of the ray and shadow queues
-                                     (per pool) */
+                                     (per pool), in [1024, 2^27] */
     int32_t shade_blocks_per_sm;  /* grid of the shading kernel (blocks of 128 threads per SM) */
     int32_t use_graph;            /* 1: replay a captured CUDA graph (a wave, or two stream
                                      iterations); 0: direct launches */
@@ -316,8 +316,9 @@ typedef struct LmgpuBatchConfig {
 
 /* The scenes (built with a BVH layout, on the current device) must outlive
  * the batch; a scene may appear more than once. Default configuration:
- * BVH2, 2^25 paths in flight (about 8 GB of path state), 16 shading blocks
- * per SM, graphs on, fixed waves (stream mode keeps every slot busy, but its
+ * BVH2, 2^27 paths in flight (about 288 bytes of path state per path, a
+ * render allocating for min(2^27, its samples)), 16 shading blocks per SM,
+ * graphs on, fixed waves (stream mode keeps every slot busy, but its
  * recycled slots scatter path state in memory: slower on the benchmark
  * scenes); a device short of memory gets fewer paths in flight. */
 int lmgpu_batch_create(LmgpuScene* const* scenes, int32_t num_scenes, LmgpuBatch** out);

@@ -74,7 +74,7 @@ struct LmgpuBatch {
     int device = 0;
     int sms = 148;
     std::vector<LmgpuScene*> scenes;
-    LmgpuBatchConfig cfg{ LMGPU_LAYOUT_BVH2, 1 << 25, 16, 1, LMGPU_BATCH_WAVES, 0 };
+    LmgpuBatchConfig cfg{ LMGPU_LAYOUT_BVH2, 1 << 27, 16, 1, LMGPU_BATCH_WAVES, 0 };
 
     BatchEntry* d_table = nullptr;
     int64_t* d_begins = nullptr;
@@ -708,7 +708,7 @@ int check_config(const LmgpuBatchConfig& c)
 {
     if (c.layout != LMGPU_LAYOUT_BVH2 && c.layout != LMGPU_LAYOUT_BVH4)
         return fail(LMGPU_ERR_INVALID, "batch layout must be LMGPU_LAYOUT_BVH2 or LMGPU_LAYOUT_BVH4");
-    if (c.wave_paths < 1024 || c.wave_paths > (1 << 26)) return fail(LMGPU_ERR_INVALID, "wave_paths must be in [1024, 2^26]");
+    if (c.wave_paths < 1024 || c.wave_paths > (1 << 27)) return fail(LMGPU_ERR_INVALID, "wave_paths must be in [1024, 2^27]");
     if (c.shade_blocks_per_sm < 1 || c.shade_blocks_per_sm > 64) return fail(LMGPU_ERR_INVALID, "shade_blocks_per_sm must be in [1, 64]");
     if (c.mode != LMGPU_BATCH_WAVES && c.mode != LMGPU_BATCH_STREAM && c.mode != LMGPU_BATCH_OVERLAP)
         return fail(LMGPU_ERR_INVALID, "unknown batch mode");
@@ -945,7 +945,7 @@ int lmgpu_batch_autotune(LmgpuBatch* b, const LmgpuRenderParams* params, double 
         if ((rc = trial(c, t)) == LMGPU_OK && t < best_t) { best = c; best_t = t; }
     }
     const int layouts[] = { LMGPU_LAYOUT_BVH2, LMGPU_LAYOUT_BVH4 };
-    const int waves[] = { 1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25 };
+    const int waves[] = { 1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25, 1 << 26, 1 << 27 };
     const int grids[] = { 4, 8, 16 };
     for (int l : layouts) {
         if (rc != LMGPU_OK || l == best.layout) continue;

@@ -99,11 +99,12 @@ void launch_full(const LmgpuScene* sc, const float* rays, int64_t n, int32_t* id
 // ------------------------------------------------------------ driver ------
 
 // Wave workspace (scratch), one per device, grown on demand.
-// Default paths per wave (32M: 7.2 GB of path state). Each bounce launch
-// ends with a latency-bound tail of the wave's longest rays, so fewer,
-// larger waves keep the GPU busier: on the 1080p terrain, waves of 4M, 8M,
-// 16M and 32M paths gave 0.94, 1.20, 1.40 and 1.53 Grays/s.
-constexpr int64_t DEFAULT_WAVE_PATHS = int64_t(1) << 25;
+// Default paths per wave (128M: 29 GB of path state; a render allocates
+// for min(wave, its samples)). Each bounce launch ends with a
+// latency-bound tail of the wave's longest rays, so fewer, larger waves
+// keep the GPU busier: on the 1080p terrain (64 spp, one 128M-path wave),
+// waves of 32M, 64M and 128M paths took 208.6, 196.8 and 189.5 ms a frame.
+constexpr int64_t DEFAULT_WAVE_PATHS = int64_t(1) << 27;
 constexpr int64_t MIN_DEFAULT_WAVE_PATHS = int64_t(1) << 20;
 
 struct Workspace {

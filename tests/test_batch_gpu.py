@@ -174,7 +174,7 @@ def test_batch_autotune_keeps_results(cuda):
     cfg = batch.autotune([r for _, r, _ in items], [n for _, _, n in items], sample_fraction=0.25)
     assert cfg["layout"] in ("bvh", "qbvh") and cfg["trial_ms"] > 0 and cfg["mode"] in ("waves", "stream", "overlap")
     assert 0 <= cfg["overlap_bounce"] <= 5
-    assert cfg["wave_paths"] in (1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25)
+    assert cfg["wave_paths"] in (1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25, 1 << 26, 1 << 27)
     assert_same(batch_films(batch, items), want)
     batch.close()
 
