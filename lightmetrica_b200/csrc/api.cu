@@ -405,6 +405,7 @@ __device__ __forceinline__ void store_hit(const LmgpuHitsSoA& hits, int64_t i, c
 
 // I/O policy of the intersection API: SoA or AoS rays in, hit arrays out.
 struct ApiHitIO {
+    static constexpr int MIN_BLOCKS = LMGPU_TRACE_API_MIN_BLOCKS;
     RaySrc rays;
     int64_t n;
     LmgpuHitsSoA hits;

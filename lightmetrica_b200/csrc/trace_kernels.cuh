@@ -24,6 +24,15 @@ namespace lmgpu {
 #ifndef LMGPU_TRACE_MIN_BLOCKS
 #define LMGPU_TRACE_MIN_BLOCKS 10     // minimum resident blocks of 128 threads per SM (48 registers)
 #endif
+// Rays of many scenes keep their scene's node and triangle pointers per lane:
+// at 10 blocks (48 registers) that spilled, at 9 (56 registers) it does not,
+// and the 64-scene batch ran 939 -> 897 ms (8 blocks: 926 ms).
+#ifndef LMGPU_TRACE_TABLE_MIN_BLOCKS
+#define LMGPU_TRACE_TABLE_MIN_BLOCKS 9
+#endif
+#ifndef LMGPU_TRACE_API_MIN_BLOCKS
+#define LMGPU_TRACE_API_MIN_BLOCKS 9   // intersection API: 2^24-ray soup 2,776 -> 2,837 Mrays/s against 10
+#endif
 #ifndef LMGPU_TRACE_SHARED_STACK
 #define LMGPU_TRACE_SHARED_STACK 12   // stack entries per lane kept in shared memory (0: none)
 #endif
@@ -42,6 +51,15 @@ template <class IO, class = void>
 struct refill_min : std::integral_constant<int, LMGPU_TRACE_REFILL_MIN> {};
 template <class IO>
 struct refill_min<IO, std::void_t<decltype(IO::REFILL_MIN)>> : std::integral_constant<int, IO::REFILL_MIN> {};
+
+// Resident blocks of 128 threads per SM the kernel is bounded to (its
+// register budget): an I/O policy may declare MIN_BLOCKS; rays of many
+// scenes default to LMGPU_TRACE_TABLE_MIN_BLOCKS.
+template <class IO, class = void>
+struct min_blocks
+    : std::integral_constant<int, per_ray_scene<IO>::value ? LMGPU_TRACE_TABLE_MIN_BLOCKS : LMGPU_TRACE_MIN_BLOCKS> {};
+template <class IO>
+struct min_blocks<IO, std::void_t<decltype(IO::MIN_BLOCKS)>> : std::integral_constant<int, IO::MIN_BLOCKS> {};
 
 // Pause threshold of a descent: an I/O policy may declare EXIT_BELOW.
 template <class IO, class = void>
@@ -79,8 +97,8 @@ __device__ __forceinline__ bool descend(const LaneScene& s, TravState& ts, Stack
 // For a multi-scene I/O policy each lane switches to its new ray's scene at
 // refill (node and triangle arrays, root); an empty scene is a miss.
 template <int LAYOUT, int STACK, bool ANY_HIT, class IO>
-__global__ void __launch_bounds__(128, LMGPU_TRACE_MIN_BLOCKS) k_trace_persistent(const DeviceScene s, const IO io, int32_t* status,
-                                                          unsigned long long* next_ray)
+__global__ void __launch_bounds__(128, min_blocks<IO>::value)
+k_trace_persistent(const DeviceScene s, const IO io, int32_t* status, unsigned long long* next_ray)
 {
     constexpr unsigned FULL = 0xffffffffu;
 #if LMGPU_TRACE_SHARED_STACK > 0
