@@ -24,10 +24,10 @@ CUDA); there is no CPU fallback.
 from .scene import (AreaLight, ConstantEnvironmentLight, DiffuseBSDF, DiffuseMirrorBSDF, HDRBitmapFilm,
                     PerfectMirrorBSDF, PerspectiveCamera, Primitive, Primitives, Scene, TriangleMesh,
                     create_scene)
-from .render import RenderProcessScheduler, Renderer, create_renderer, create_scheduler
+from .render import RenderProcessScheduler, Renderer, create_renderer, create_scheduler, release_render_memory
 from . import native
 
 __all__ = ["AreaLight", "ConstantEnvironmentLight", "DiffuseBSDF", "DiffuseMirrorBSDF", "HDRBitmapFilm",
            "PerfectMirrorBSDF", "PerspectiveCamera", "Primitive", "Primitives", "Scene", "TriangleMesh",
            "create_scene", "Renderer", "RenderProcessScheduler", "create_renderer", "create_scheduler",
-           "native"]
+           "release_render_memory", "native"]

@@ -512,4 +512,28 @@ int lmgpu_render(LmgpuScene* scene, const LmgpuRenderParams* params, float* film
     return LMGPU_OK;
 }
 
+int lmgpu_render_release(void)
+{
+    int dev = 0;
+    LMGPU_CUDA_TRY(cudaGetDevice(&dev));
+    {
+        // Takes the lock a render holds until its device work is done.
+        DeviceWorkspace& dw = device_workspace(dev);
+        std::lock_guard<std::mutex> lock(dw.mu);
+        if (dw.ws.mem) LMGPU_CUDA_TRY(cudaFree(dw.ws.mem));
+        dw.ws.mem = nullptr;
+        dw.ws.capacity = 0;
+    }
+    HostFilmBuffers& hb = host_film_buffers(dev);
+    std::lock_guard<std::mutex> lock(hb.mu);
+    if (hb.film) LMGPU_CUDA_TRY(cudaFree(hb.film));
+    if (hb.out) LMGPU_CUDA_TRY(cudaFree(hb.out));
+    if (hb.pinned) LMGPU_CUDA_TRY(cudaFreeHost(hb.pinned));
+    hb.film = nullptr;
+    hb.out = nullptr;
+    hb.pinned = nullptr;
+    hb.film_bytes = hb.out_bytes = 0;
+    return LMGPU_OK;
+}
+
 }  // extern "C"

@@ -119,6 +119,7 @@ SIGNATURES = {
     "lmgpu_render": (c_int32, [c_void_p, P(RenderParams), c_void_p, P(RenderStats)]),
     "lmgpu_render_device": (c_int32, [c_void_p, P(RenderParams), c_void_p, c_void_p, P(RenderStats)]),
     "lmgpu_render_device_noalloc": (c_int32, [c_void_p, P(RenderParams), c_void_p, c_void_p]),
+    "lmgpu_render_release": (c_int32, []),
     "lmgpu_scene_status": (c_int32, [c_void_p, c_void_p]),
     "lmgpu_adjoint_forward": (c_int32, [c_void_p, P(RenderParams), P(DiffParams), c_void_p, c_void_p, P(RenderStats)]),
     "lmgpu_adjoint_backward": (c_int32, [c_void_p, P(RenderParams), P(DiffParams), c_void_p, c_void_p, c_void_p,

@@ -176,6 +176,14 @@ class RenderProcessScheduler:
         return film
 
 
+def release_render_memory() -> None:
+    """Frees the device memory renders keep between calls on the current
+    device (the wave workspace: 216 bytes per path of the largest wave so far,
+    28.7 GB after a 1080p 64-spp frame; lmgpu_render's film buffers). The
+    next render allocates it again."""
+    N.check(N.lib().lmgpu_render_release())
+
+
 def create_renderer(impl: str = "pt") -> Renderer:
     return Renderer(impl)
 

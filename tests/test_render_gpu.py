@@ -75,6 +75,19 @@ def test_layouts_and_fp64_film_agree(cuda):
     np.testing.assert_allclose(a, c, rtol=1e-9, atol=1e-9)
 
 
+def test_release_render_memory_then_render_again(cuda):
+    """lmgpu_render_release frees the cached workspace and film buffers; a
+    second release is harmless and the next render allocates again and
+    renders the same paths."""
+    from lightmetrica_b200 import release_render_memory
+    prims = scenes.cornell_box(64, 64, variant="mixed")
+    a, _ = render(prims, "pt.mis", 256, fp64=True)
+    release_render_memory()
+    release_render_memory()
+    b, _ = render(prims, "pt.mis", 256, fp64=True)
+    np.testing.assert_allclose(a, b, rtol=1e-9, atol=1e-9)
+
+
 def test_max_path_vertices_edges(cuda):
     prims = scenes.cornell_box(64, 64)
     black, _ = render(prims, "pt", 16, max_pv=1)
