@@ -248,7 +248,7 @@ int lmgpu_render_release(void);
  * manager that forbids allocations, code running during CUDA stream
  * capture, a process at its memory budget. The wave workspace (path state
  * and queues) lives in a static 32 MiB device array that every GPU loading
- * the library holds until exit; waves are at most 190,650 paths, and a
+ * the library holds until exit; waves are at most 155,343 paths, and a
  * `wave_paths` above that returns LMGPU_ERR_INVALID (0 = the maximum). The
  * scene, created beforehand, and the DEVICE film (float, or double with
  * film_fp64; accumulated, not rescaled; the caller zeroes it) are the

@@ -17,7 +17,7 @@ namespace lmgpu {
 namespace {
 
 // Size of the static workspace: every GPU that loads this module holds it
-// until the process exits. 32 MiB gives waves of 190,650 paths.
+// until the process exits. 32 MiB gives waves of 155,343 paths.
 constexpr size_t NOALLOC_WORKSPACE_BYTES = size_t(32) << 20;
 
 __device__ __align__(256) unsigned char g_noalloc_workspace[NOALLOC_WORKSPACE_BYTES];
