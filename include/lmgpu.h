@@ -245,18 +245,18 @@ int lmgpu_render_release(void);
  * cudaMalloc, cudaFree or allocating library routine. It has no counterpart
  * in the reference. It is for callers that cannot allocate device memory
  * while rendering: a host application's render callback under a memory
- * manager that forbids allocations, code running during CUDA stream
- * capture, a process at its memory budget. The wave workspace (path state
- * and queues) lives in a static 32 MiB device array that every GPU loading
- * the library holds until exit; waves are at most 155,343 paths, and a
- * `wave_paths` above that returns LMGPU_ERR_INVALID (0 = the maximum). The
- * scene, created beforehand, and the DEVICE film (float, or double with
- * film_fp64; accumulated, not rescaled; the caller zeroes it) are the
- * caller's. The first call on each device looks up the array's device
- * address, so make it before any stream capture. All calls share the one
- * array, and the counters in it are cleared at the start of each wave, but
- * calls that overlap on the GPU race: run them one after another. The call
- * synchronises `stream`. */
+ * manager that forbids allocations, a process at its memory budget. The wave
+ * workspace (path state and queues) lives in a static 32 MiB device array
+ * that every GPU loading the library holds until exit; waves are at most
+ * 155,343 paths, and a `wave_paths` above that returns LMGPU_ERR_INVALID
+ * (0 = the maximum). The scene, created beforehand, and the DEVICE film
+ * (float, or double with film_fp64; accumulated, not rescaled; the caller
+ * zeroes it) are the caller's. The first call on each device looks up the
+ * array's device address, so make it before any stream capture. All calls
+ * share the one array, and the counters in it are cleared at the start of
+ * each wave, but calls that overlap on the GPU race: run them one after
+ * another. Like lmgpu_render_device, the call reads each bounce's queue
+ * sizes back to the host, so it synchronises `stream` after every bounce. */
 int lmgpu_render_device_noalloc(LmgpuScene* scene, const LmgpuRenderParams* params,
                                 void* film_device, void* stream);
 

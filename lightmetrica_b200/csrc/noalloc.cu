@@ -3,10 +3,11 @@
 // lmgpu_render_device caches its wavefront workspace (path state, ray and
 // shadow queues) in memory it allocates with cudaMalloc on first use. Some
 // callers cannot allow that: a render callback of a host application whose
-// memory manager forbids device allocations, code that runs while a CUDA
-// stream is being captured, or a process already at its memory budget. This
-// entry point runs the same waves over a fixed workspace that lives in this
-// file's static device array instead, so a call allocates nothing.
+// memory manager forbids device allocations, or a process already at its
+// memory budget. This entry point runs the same waves over a fixed workspace
+// that lives in this file's static device array instead, so a call allocates
+// nothing. Like lmgpu_render_device, it reads each bounce's queue sizes back
+// to the host, so it synchronises its stream after every bounce.
 #include <cuda_runtime.h>
 #include <mutex>
 

@@ -516,23 +516,32 @@ int lmgpu_render_release(void)
 {
     int dev = 0;
     LMGPU_CUDA_TRY(cudaGetDevice(&dev));
+    // Every field is reset whatever its free returns, so no later render
+    // reuses (or frees again) memory that this call handed back; the first
+    // failure is reported once all of them are reset.
+    cudaError_t first = cudaSuccess;
+    const char* what = nullptr;
+    auto note = [&](cudaError_t e, const char* w) {
+        if (e != cudaSuccess && first == cudaSuccess) { first = e; what = w; }
+    };
     {
         // Takes the lock a render holds until its device work is done.
         DeviceWorkspace& dw = device_workspace(dev);
         std::lock_guard<std::mutex> lock(dw.mu);
-        if (dw.ws.mem) LMGPU_CUDA_TRY(cudaFree(dw.ws.mem));
+        if (dw.ws.mem) note(cudaFree(dw.ws.mem), "cudaFree(workspace)");
         dw.ws.mem = nullptr;
         dw.ws.capacity = 0;
     }
     HostFilmBuffers& hb = host_film_buffers(dev);
     std::lock_guard<std::mutex> lock(hb.mu);
-    if (hb.film) LMGPU_CUDA_TRY(cudaFree(hb.film));
-    if (hb.out) LMGPU_CUDA_TRY(cudaFree(hb.out));
-    if (hb.pinned) LMGPU_CUDA_TRY(cudaFreeHost(hb.pinned));
+    if (hb.film) note(cudaFree(hb.film), "cudaFree(film)");
+    if (hb.out) note(cudaFree(hb.out), "cudaFree(rescaled film)");
+    if (hb.pinned) note(cudaFreeHost(hb.pinned), "cudaFreeHost(film copy)");
     hb.film = nullptr;
     hb.out = nullptr;
     hb.pinned = nullptr;
     hb.film_bytes = hb.out_bytes = 0;
+    if (first != cudaSuccess) return cuda_fail(first, what);
     return LMGPU_OK;
 }
 

@@ -28,15 +28,32 @@ _I = ctypes.c_int
 _LL = ctypes.c_longlong
 
 
-def build(reference_root: str = "/root/reference") -> None:
-    """Compile the C restatement and, when the reference tree is present, the
-    reference harness (oracle/_ref) and the product's lightmetrica plugin
-    built against the reference headers (oracle/_ref/plugin.gpu.so).
-    Building the checker is not using it."""
+def reference_root(required: bool = False):
+    """The lightmetrica source tree named by the environment variable
+    LM_REFERENCE_ROOT (a checkout of hi2p-perim/lightmetrica), or None when it
+    is unset. With `required`, an unset or wrong variable raises."""
+    root = os.environ.get("LM_REFERENCE_ROOT")
+    ok = bool(root) and os.path.isdir(os.path.join(root, "src", "liblightmetrica"))
+    if required and not ok:
+        raise RuntimeError("set LM_REFERENCE_ROOT to a lightmetrica source tree (it holds src/liblightmetrica); "
+                           f"got {root!r}")
+    return root if ok else None
+
+
+def build(reference_root_dir: str | None = None) -> None:
+    """Compile the C restatement and, when a reference tree is given (the
+    argument, or LM_REFERENCE_ROOT), the reference harness (oracle/_ref) and
+    the product's lightmetrica plugin built against the reference headers
+    (oracle/_ref/plugin.gpu.so). Without one, oracle/_ref keeps what an
+    earlier build left there. Building the checker is not using it."""
     subprocess.run(["bash", os.path.join(HERE, "build_oracle.sh")], check=True)
-    if os.path.isdir(os.path.join(reference_root, "src", "liblightmetrica")):
-        subprocess.run(["bash", os.path.join(HERE, "build_ref.sh"), reference_root], check=True)
-        subprocess.run(["bash", os.path.join(HERE, "build_plugin.sh"), reference_root], check=True)
+    root = reference_root_dir or reference_root()
+    if root and os.path.isdir(os.path.join(root, "src", "liblightmetrica")):
+        subprocess.run(["bash", os.path.join(HERE, "build_ref.sh"), root], check=True)
+        subprocess.run(["bash", os.path.join(HERE, "build_plugin.sh"), root], check=True)
+    else:
+        print("oracle: LM_REFERENCE_ROOT is unset (or holds no src/liblightmetrica); "
+              "oracle/_ref not rebuilt", flush=True)
 
 
 def _ptr(a):

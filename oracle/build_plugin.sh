@@ -10,11 +10,15 @@
 # and to liblmgpu.so. Output: oracle/_ref/plugin.gpu.so. -Bsymbolic keeps the
 # plugin's own plugin registry (plugin.common.cpp) inside the plugin.
 #
-# Usage: oracle/build_plugin.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_plugin.sh [REFERENCE_ROOT]   (default: $LM_REFERENCE_ROOT)
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
 ROOT="$(dirname "$HERE")"
-REF="${1:-/root/reference}"
+REF="${1:-${LM_REFERENCE_ROOT:-}}"
+if [ -z "$REF" ]; then
+  echo "no reference tree: pass REFERENCE_ROOT or set LM_REFERENCE_ROOT" >&2
+  exit 2
+fi
 OUT="$HERE/_ref"
 if [ ! -d "$REF/src/liblightmetrica" ] || [ ! -f "$OUT/liblmref_f.so" ] || [ ! -f "$ROOT/lightmetrica_b200/_lib/liblmgpu.so" ]; then
   echo "reference tree, oracle/_ref/liblmref_f.so or liblmgpu.so missing; skipping plugin.gpu.so" >&2

@@ -11,10 +11,14 @@
 # the QBVH source needs -fno-strict-aliasing on GCC 13, without it
 # it returns no hits. Nothing is written outside oracle/_ref.
 #
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default: $LM_REFERENCE_ROOT)
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${LM_REFERENCE_ROOT:-}}"
+if [ -z "$REF" ]; then
+  echo "no reference tree: pass REFERENCE_ROOT or set LM_REFERENCE_ROOT" >&2
+  exit 2
+fi
 OUT="$HERE/_ref"
 if [ ! -d "$REF/src/liblightmetrica" ]; then
   echo "reference tree not found at $REF; skipping oracle/_ref build" >&2

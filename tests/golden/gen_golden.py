@@ -1,8 +1,9 @@
 """Generates the golden fixtures in this directory from the reference's own
 code (oracle/_ref, built from the reference sources by oracle/build_ref.sh).
 
-Run from the repository root in a container that has the reference tree:
-    python tests/golden/gen_golden.py
+Run from the repository root, with LM_REFERENCE_ROOT naming the reference
+source tree (oracle/_ref is built from it first):
+    LM_REFERENCE_ROOT=<lightmetrica checkout> python tests/golden/gen_golden.py
 
 Fixtures:
   intersect_simple.npz     reference test Intersect_Simple
@@ -172,7 +173,7 @@ def terrain_image(spp: int = 16384):
     print("wrote terrain image", f"{spp} spp {secs:.1f} s", film.mean(axis=(0, 1)))
 
 
-def scene_literals(reference_root: str = "/root/reference"):
+def scene_literals(reference_root: str | None = None):
     """The XML scene literals of the reference's own Primitives and BPT tests
     (test.primitives.cpp: SceneNode_Success, _WithTransformByMatrix,
     _WithTransform; test.bpt.mis.cpp: SceneFile), extracted verbatim as test
@@ -180,6 +181,7 @@ def scene_literals(reference_root: str = "/root/reference"):
     reference assertions they restate."""
     import json
     import re
+    reference_root = reference_root or oracle.reference_root(required=True)
     out = {}
     for fname, names in (("test.primitives.cpp", ("SceneNode_Success", "SceneNode_Success_WithTransformByMatrix",
                                                    "SceneNode_Success_WithTransform")),
