@@ -108,6 +108,11 @@ typedef struct {
     int32_t film_height;
     int32_t layout;             /* LMGPU_LAYOUT_* */
     int32_t build_threads;      /* host threads for the BVH build, 0 = all */
+    int32_t max_stack_entries;  /* traversal stack bound per ray, 0 = automatic (2 * tree depth + 4,
+                                   enough for every walk); a smaller bound makes the walks that
+                                   need more fail with LMGPU_ERR_STACK_OVERFLOW (the status word
+                                   the kernels raise). The multi-scene batch always uses the
+                                   largest compiled bound. */
 } LmgpuSceneDesc;
 
 typedef struct {
@@ -342,6 +347,34 @@ int lmgpu_batch_set_config(LmgpuBatch* batch, const LmgpuBatchConfig* config);
  * in which case the call synchronises and fills the totals of the batch. */
 int lmgpu_batch_render_device(LmgpuBatch* batch, const LmgpuRenderParams* params,
                               void* const* films_device, void* stream, LmgpuRenderStats* stats);
+
+/* Host-film variant: renders every scene like lmgpu_batch_render_device and
+ * writes each scene's rescaled film (W*H*3 floats, the reference's
+ * Rescale(W*H/num_samples), sched.mt.cpp:250-256) to the HOST buffer
+ * films_host[i]: the batch counterpart of lmgpu_render. The batch keeps its
+ * device films, their rescaled copies and a pinned host copy between calls
+ * (about 3 * 12 bytes per pixel over all scenes for float films). Uses the
+ * legacy default stream; synchronises. */
+int lmgpu_batch_render(LmgpuBatch* batch, const LmgpuRenderParams* params, float* const* films_host,
+                       LmgpuRenderStats* stats);
+
+/* Measurement of one batch render (no counterpart in the reference). The
+ * batch renders with direct launches in fixed waves (no graph; its
+ * configuration is otherwise kept), records CUDA events on `stream` around
+ * every traversal launch and, with count_tests, counts each traversal's
+ * binary-node slab tests (four per 4-wide node) and TriAccel tests with a
+ * counting copy of the traversal kernel, whose times are then not the
+ * render's. Films as lmgpu_batch_render_device; synchronises. */
+typedef struct {
+    int64_t rays[2];            /* [0] closest-hit (path) rays, [1] shadow rays */
+    int64_t launches[2];        /* traversal launches of each kind */
+    double trace_ms[2];         /* summed device time of those launches */
+    double render_ms;           /* device time of the whole render */
+    uint64_t node_tests[2];     /* count_tests only: slab tests per kind */
+    uint64_t tri_tests[2];      /* count_tests only: TriAccel tests per kind */
+} LmgpuTraceProfile;
+int lmgpu_batch_profile(LmgpuBatch* batch, const LmgpuRenderParams* params, void* const* films_device,
+                        void* stream, int32_t count_tests, LmgpuTraceProfile* profile);
 
 /* Autotuner: renders the batch with each scene's sample count scaled by
  * `sample_fraction` (0 < f <= 1; raised for a candidate until the trial

@@ -73,53 +73,83 @@ class SceneBatch:
         N.check(N.lib().lmgpu_batch_set_config(self.handle, ctypes.byref(c)))
 
     # ------------------------------------------------------------ render --
-    def _params(self, renderers, num_samples, film_fp64):
+    def _params(self, renderers, num_samples, film_fp64, sample_offsets=None):
         n = len(self.scenes)
         if isinstance(renderers, Renderer):
             renderers = [renderers] * n
         if np.isscalar(num_samples):
             num_samples = [int(num_samples)] * n
-        if len(renderers) != n or len(num_samples) != n:
-            raise ValueError("one renderer and one sample count per scene")
+        if sample_offsets is None or np.isscalar(sample_offsets):
+            sample_offsets = [int(sample_offsets or 0)] * n
+        if len(renderers) != n or len(num_samples) != n or len(sample_offsets) != n:
+            raise ValueError("one renderer, one sample count and one sample offset per scene")
         arr = (N.RenderParams * n)()
-        for i, (r, k) in enumerate(zip(renderers, num_samples)):
-            arr[i] = r.params(int(k), film_fp64=film_fp64)
+        for i, (r, k, o) in enumerate(zip(renderers, num_samples, sample_offsets)):
+            arr[i] = r.params(int(k), sample_offset=int(o), film_fp64=film_fp64)
         return arr
 
-    def render_device(self, renderers, num_samples, films, stream=None, stats: bool = True):
+    @staticmethod
+    def _stats(st):
+        return {"rays_traced": st.rays_traced, "shadow_rays": st.shadow_rays, "paths": st.paths,
+                "waves": st.waves, "max_bounces_run": st.max_bounces_run, "device_ms": st.device_ms}
+
+    def render_device(self, renderers, num_samples, films, stream=None, stats: bool = True, sample_offsets=None):
         """Accumulates each scene's un-rescaled samples into `films[i]`
-        (CUDA tensors of W*H*3 float32, or float64 with film_fp64)."""
+        (CUDA tensors of W*H*3 float32, or float64 with film_fp64);
+        `sample_offsets` gives each scene's first sample index (default 0)."""
         import torch
         fp64 = films[0].dtype == torch.float64
-        params = self._params(renderers, num_samples, fp64)
+        params = self._params(renderers, num_samples, fp64, sample_offsets)
         ptrs = (ctypes.c_void_p * len(films))(*[f.data_ptr() for f in films])
         s = stream if stream is not None else torch.cuda.current_stream(films[0].device).cuda_stream
         st = N.RenderStats() if stats else None
         N.check(N.lib().lmgpu_batch_render_device(self.handle, params, ptrs, ctypes.c_void_p(s),
                                                   ctypes.byref(st) if stats else None))
         if stats:
-            self.last_stats = {"rays_traced": st.rays_traced, "shadow_rays": st.shadow_rays, "paths": st.paths,
-                               "waves": st.waves, "max_bounces_run": st.max_bounces_run, "device_ms": st.device_ms}
+            self.last_stats = self._stats(st)
         return films
 
-    def render(self, renderers, num_samples, film_fp64: bool = False):
-        """Renders every scene; returns the rescaled films (H, W, 3) as numpy
-        arrays (the reference's Rescale(W * H / num_samples))."""
-        import torch
+    def render(self, renderers, num_samples, film_fp64: bool = False, sample_offsets=None, out=None):
+        """Renders every scene through lmgpu_batch_render; returns the
+        rescaled films (H, W, 3) float32 (the reference's Rescale(W * H /
+        num_samples)). `out` may give the host arrays to fill."""
         n = len(self.scenes)
-        if np.isscalar(num_samples):
-            num_samples = [int(num_samples)] * n
-        dt = torch.float64 if film_fp64 else torch.float32
-        films = []
-        for s in self.scenes:
+        params = self._params(renderers, num_samples, film_fp64, sample_offsets)
+        if out is None:
+            out = []
+            for s in self.scenes:
+                cam = s.main_camera()
+                out.append(np.empty((cam.film.height, cam.film.width, 3), np.float32))
+        for s, f in zip(self.scenes, out):
             cam = s.main_camera()
-            films.append(torch.zeros(cam.film.width * cam.film.height * 3, dtype=dt, device="cuda"))
-        self.render_device(renderers, num_samples, films)
-        out = []
-        for s, f, k in zip(self.scenes, films, num_samples):
-            cam = s.main_camera()
-            W, H = cam.film.width, cam.film.height
-            out.append((f.double() * (W * H / k)).float().cpu().numpy().reshape(H, W, 3))
+            if f.dtype != np.float32 or f.size != cam.film.width * cam.film.height * 3 or not f.flags.c_contiguous:
+                raise ValueError("each output film must be a C-contiguous float32 array of W*H*3 values")
+        ptrs = (ctypes.c_void_p * n)(*[f.ctypes.data for f in out])
+        st = N.RenderStats()
+        N.check(N.lib().lmgpu_batch_render(self.handle, params, ptrs, ctypes.byref(st)))
+        self.last_stats = self._stats(st)
+        return out
+
+    def profile(self, renderers, num_samples, films, count_tests: bool = False, stream=None,
+                sample_offsets=None) -> dict:
+        """One measurement render (lmgpu_batch_profile): direct launches in
+        fixed waves with CUDA events around every traversal launch; with
+        `count_tests`, the slab and TriAccel tests of every ray (counting
+        kernels: their times are not the render's)."""
+        import torch
+        fp64 = films[0].dtype == torch.float64
+        params = self._params(renderers, num_samples, fp64, sample_offsets)
+        ptrs = (ctypes.c_void_p * len(films))(*[f.data_ptr() for f in films])
+        s = stream if stream is not None else torch.cuda.current_stream(films[0].device).cuda_stream
+        p = N.TraceProfile()
+        N.check(N.lib().lmgpu_batch_profile(self.handle, params, ptrs, ctypes.c_void_p(s), 1 if count_tests else 0,
+                                            ctypes.byref(p)))
+        out = {"render_ms": p.render_ms}
+        for k, name in ((0, "closest"), (1, "shadow")):
+            out[name] = {"rays": p.rays[k], "launches": p.launches[k], "trace_ms": p.trace_ms[k]}
+            if count_tests:
+                out[name]["node_tests"] = int(p.node_tests[k])
+                out[name]["tri_tests"] = int(p.tri_tests[k])
         return out
 
     def autotune(self, renderers, num_samples, sample_fraction: float = 0.125, stream=None) -> dict:

@@ -57,8 +57,8 @@ __device__ __forceinline__ int32_t cast_ray(const DeviceScene& s, V3 o, V3 d, fl
     h.tri = -1;
     if (s.num_tris == 0) return -1;
     bool ok;
-    if (LAYOUT == LMGPU_LAYOUT_BVH2) ok = trace_bvh2<ANY>(s.bvh2, s.tris, s.root_ref, s.root_box, r, h, stack, STACK, nullptr);
-    else if (LAYOUT == LMGPU_LAYOUT_BVH4) ok = trace_bvh4<ANY>(s.bvh4, s.tris, s.root_ref4, s.root_box, r, h, stack, STACK, nullptr);
+    if (LAYOUT == LMGPU_LAYOUT_BVH2) ok = trace_bvh2<ANY>(s.bvh2, s.tris, s.root_ref, s.root_box, r, h, stack, s.stack_cap < STACK ? s.stack_cap : STACK, nullptr);
+    else if (LAYOUT == LMGPU_LAYOUT_BVH4) ok = trace_bvh4<ANY>(s.bvh4, s.tris, s.root_ref4, s.root_box, r, h, stack, s.stack_cap < STACK ? s.stack_cap : STACK, nullptr);
     else { trace_naive<ANY>(s.tris_by_id, s.num_tris, r, h, nullptr); ok = true; }
     if (!ok) { atomicOr(status, STATUS_STACK_OVERFLOW); h.tri = -1; }
     return h.tri;

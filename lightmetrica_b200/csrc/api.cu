@@ -169,6 +169,7 @@ int create_impl(const LmgpuSceneDesc* desc, LmgpuScene** out)
     *out = nullptr;
     if (desc->num_primitives < 0 || (desc->num_primitives > 0 && !desc->primitives))
         return fail(LMGPU_ERR_INVALID, "bad primitive list");
+    if (desc->max_stack_entries < 0) return fail(LMGPU_ERR_INVALID, "negative traversal stack bound");
     if (desc->layout < LMGPU_LAYOUT_BVH2 || desc->layout > LMGPU_LAYOUT_NAIVE)
         return fail(LMGPU_ERR_INVALID, "unknown layout");
     for (int i = 0; i < desc->num_primitives; i++) {
@@ -210,6 +211,7 @@ int create_impl(const LmgpuSceneDesc* desc, LmgpuScene** out)
     d.root_ref = b.bvh2_root;
     d.root_ref4 = b.bvh4_root;
     d.stack_cap = 2 * b.max_depth + 4;
+    if (desc->max_stack_entries > 0 && desc->max_stack_entries < d.stack_cap) d.stack_cap = desc->max_stack_entries;
     std::memcpy(d.root_box, b.root_box, sizeof(d.root_box));
     d.cam = cam;
 
@@ -352,48 +354,6 @@ __device__ __forceinline__ RayIn load_ray(const RaySrc& R, int64_t i)
     return in;
 }
 
-template <int LAYOUT, bool ANY_HIT, int STACK>
-__device__ __forceinline__ bool trace_one(const DeviceScene& s, TraversalRay& r, Hit& h, int2* stack, TraceStats* st)
-{
-    if (s.num_tris == 0) { h.tri = -1; return true; }   // empty scene: no node arrays exist
-    if (LAYOUT == LMGPU_LAYOUT_BVH2)
-        return trace_bvh2<ANY_HIT>(s.bvh2, s.tris, s.root_ref, s.root_box, r, h, stack, STACK, st);
-    if (LAYOUT == LMGPU_LAYOUT_BVH4)
-        return trace_bvh4<ANY_HIT>(s.bvh4, s.tris, s.root_ref4, s.root_box, r, h, stack, STACK, st);
-    trace_naive<ANY_HIT>(s.tris_by_id, s.num_tris, r, h, st);
-    return true;
-}
-
-template <int LAYOUT, int STACK, bool STATS>
-__global__ void __launch_bounds__(128) k_intersect(const DeviceScene s, const RaySrc rays, int64_t n,
-                                                   const LmgpuHitsSoA hits, int32_t* status,
-                                                   unsigned long long* counters)
-{
-    int2 stack[STACK];
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    TraceStats st{ 0, 0 };
-    if (i < n) {
-        TraversalRay r;
-        setup_ray(r, load_ray(rays, i));
-        Hit h;
-        const bool ok = trace_one<LAYOUT, false, STACK>(s, r, h, stack, STATS ? &st : nullptr);
-        if (!ok) { atomicOr(status, STATUS_STACK_OVERFLOW); h.tri = -1; }
-        const bool hit = h.tri >= 0;
-        if (hits.tri_id) hits.tri_id[i] = h.tri;
-        if (hits.t) hits.t[i] = hit ? h.t : 0.0f;
-        if (hits.u) hits.u[i] = hit ? h.u : 0.0f;
-        if (hits.v) hits.v[i] = hit ? h.v : 0.0f;
-    }
-    if (STATS) {
-        unsigned long long a = st.nodes, b = st.tris;
-        for (int o = 16; o > 0; o >>= 1) {
-            a += __shfl_down_sync(0xffffffffu, a, o);
-            b += __shfl_down_sync(0xffffffffu, b, o);
-        }
-        if ((threadIdx.x & 31) == 0) { atomicAdd(counters, a); atomicAdd(counters + 1, b); }
-    }
-}
-
 __device__ __forceinline__ void store_hit(const LmgpuHitsSoA& hits, int64_t i, const Hit& h)
 {
     const bool hit = h.tri >= 0;
@@ -424,33 +384,14 @@ struct ApiAnyIO {
     __device__ void store(int64_t i, const Hit& h, const TraversalRay&) const { occluded[i] = h.tri >= 0 ? 1 : 0; }
 };
 
-template <int STACK>
-int launch_counted_stack(LmgpuScene* sc, const RaySrc& rays, int64_t n, const LmgpuHitsSoA& hits,
-                         cudaStream_t stream, unsigned long long* counters)
-{
-    const int threads = 128;
-    const int64_t blocks = (n + threads - 1) / threads;
-    const DeviceScene& s = sc->dev;
-    switch (s.layout) {
-    case LMGPU_LAYOUT_BVH2: k_intersect<LMGPU_LAYOUT_BVH2, STACK, true><<<blocks, threads, 0, stream>>>(s, rays, n, hits, sc->d_status, counters); break;
-    case LMGPU_LAYOUT_BVH4: k_intersect<LMGPU_LAYOUT_BVH4, STACK, true><<<blocks, threads, 0, stream>>>(s, rays, n, hits, sc->d_status, counters); break;
-    default: k_intersect<LMGPU_LAYOUT_NAIVE, 1, true><<<blocks, threads, 0, stream>>>(s, rays, n, hits, sc->d_status, counters); break;
-    }
-    LMGPU_CUDA_TRY(cudaGetLastError());
-    return LMGPU_OK;
-}
-
 int launch_intersect(LmgpuScene* sc, const RaySrc& rays, int64_t n, const LmgpuHitsSoA& hits,
                      cudaStream_t stream, unsigned long long* counters)
 {
     if (n == 0) return LMGPU_OK;
     if (!counters) return launch_trace<false>(sc, ApiHitIO{ rays, n, hits }, n, stream);
-    const int cap = sc->dev.stack_cap;
-    if (cap <= 32) return launch_counted_stack<32>(sc, rays, n, hits, stream, counters);
-    if (cap <= 64) return launch_counted_stack<64>(sc, rays, n, hits, stream, counters);
-    if (cap <= 128) return launch_counted_stack<128>(sc, rays, n, hits, stream, counters);
-    if (cap <= 256) return launch_counted_stack<256>(sc, rays, n, hits, stream, counters);
-    return fail(LMGPU_ERR_UNSUPPORTED, "BVH deeper than the largest compiled traversal stack (256)");
+    // The counting instantiation of the same persistent kernel the path
+    // tracer's measurement renders use.
+    return launch_trace<false, ApiHitIO, true>(sc, ApiHitIO{ rays, n, hits }, n, stream, counters);
 }
 
 // Exposed for the measurement path (traversal counters).

@@ -68,6 +68,16 @@ struct GraphKey {
     }
 };
 
+// A measurement render's record (lmgpu_batch_profile): events around every
+// traversal launch and, with `count`, the counting kernels' totals.
+struct TraceProfileRun {
+    bool count = false;
+    std::vector<cudaEvent_t> events;          // start, end of each traversal launch
+    std::vector<int> kinds;                   // 0 closest hit, 1 shadow
+    unsigned long long* d_counts = nullptr;   // [kind][slab tests, TriAccel tests]
+    cudaError_t error = cudaSuccess;
+};
+
 }  // namespace
 
 struct LmgpuBatch {
@@ -105,11 +115,28 @@ struct LmgpuBatch {
     cudaGraphExec_t exec_head = nullptr;    // overlap: pool 0's first head
     cudaGraphExec_t exec_tail = nullptr;    // overlap: pool 0's last tail
     GraphKey key;
+
+    TraceProfileRun* prof = nullptr;        // set during lmgpu_batch_profile only
+
+    // lmgpu_batch_render's films: device films of all scenes, their rescaled
+    // float copies and a pinned host copy.
+    void* hf_film = nullptr;
+    size_t hf_film_bytes = 0;
+    float* hf_out = nullptr;
+    float* hf_pinned = nullptr;
+    size_t hf_out_bytes = 0;
 };
 
 namespace {
 
 // ------------------------------------------------------ small kernels ----
+
+template <class F>
+__global__ void k_rescale_film(const F* film, float* out, int64_t n, double scale)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (float)((double)film[i] * scale);
+}
 
 // Pool l starts at wave l; each pool then advances by `pools` waves.
 __global__ void k_batch_setup(WaveCtl* wave, int pools, int64_t total, int64_t step, unsigned long long* stats)
@@ -207,6 +234,33 @@ __global__ void k_stream_plan(StreamCtl* ctl, uint32_t* counters, int q, unsigne
 
 // ------------------------------------------------------- wave builder ----
 
+// Launches one persistent traversal of `io`. During a measurement render
+// (b->prof) the launch is bracketed by CUDA events and, when counting, runs
+// the counting instantiation of the same kernel.
+template <int LAYOUT, int STACK, bool ANY_HIT, class IO>
+void launch_traversal(const LmgpuBatch* b, int blocks, const DeviceScene& proto, const IO& io,
+                      unsigned long long* work, cudaStream_t s)
+{
+    TraceProfileRun* p = b->prof;
+    if (!p) {
+        k_trace_persistent<LAYOUT, STACK, ANY_HIT, IO><<<blocks, 128, 0, s>>>(proto, io, b->d_status, work, nullptr);
+        return;
+    }
+    cudaEvent_t e[2] = { nullptr, nullptr };
+    for (cudaEvent_t& x : e)
+        if (p->error == cudaSuccess) p->error = cudaEventCreate(&x);
+    if (p->error == cudaSuccess) p->error = cudaEventRecord(e[0], s);
+    if (p->count)
+        k_trace_persistent<LAYOUT, STACK, ANY_HIT, IO, true><<<blocks, 128, 0, s>>>(
+            proto, io, b->d_status, work, p->d_counts + (ANY_HIT ? 2 : 0));
+    else
+        k_trace_persistent<LAYOUT, STACK, ANY_HIT, IO><<<blocks, 128, 0, s>>>(proto, io, b->d_status, work, nullptr);
+    if (p->error == cudaSuccess) p->error = cudaEventRecord(e[1], s);
+    for (cudaEvent_t x : e)
+        if (x) p->events.push_back(x);
+    if (e[0] && e[1]) p->kinds.push_back(ANY_HIT ? 1 : 0);
+}
+
 struct Launch {
     int64_t paths;             // wave capacity
     int shade_blocks;
@@ -238,8 +292,7 @@ struct Wave {
     {
         const PathState& st = b->st[l];
         ShadowIO<FilmCtx> io{ st.counters + 2, st.sh_o, st.sh_d, st.sh_c, st.L, film_ctx(b, l) };
-        k_trace_persistent<LAYOUT, STACK, true, ShadowIO<FilmCtx>><<<L.shadow_blocks, 128, 0, s>>>(
-            L.proto, io, b->d_status, work(b, l) + slot);
+        launch_traversal<LAYOUT, STACK, true>(b, L.shadow_blocks, L.proto, io, work(b, l) + slot, s);
     }
 
     static void bounce(const LmgpuBatch* b, const Launch& L, int l, int k, int slot, cudaStream_t s)
@@ -248,8 +301,7 @@ struct Wave {
         const int qin = (k - 1) & 1;
         k_bounce_prep<<<1, 1, 0, s>>>(st.counters, qin, k, b->d_stats);
         PathRayIO<true> io{ st.counters + qin, st.qo[qin], st.qd[qin], st.hit, b->d_table };
-        k_trace_persistent<LAYOUT, STACK, false, PathRayIO<true>><<<L.trace_blocks, 128, 0, s>>>(
-            L.proto, io, b->d_status, work(b, l) + slot);
+        launch_traversal<LAYOUT, STACK, false>(b, L.trace_blocks, L.proto, io, work(b, l) + slot, s);
         k_pt_shade<TECH, Ctx><<<L.shade_blocks, 128, 0, s>>>(ctx(b, l), st, k, qin, 1 - qin);
         if (TECH != LMGPU_RENDER_PT) shadow(b, L, l, slot + 1, s);
     }
@@ -308,13 +360,11 @@ struct Stream {
         k_stream_plan<<<1, 1, 0, s>>>(b->d_ctl, st.counters, q, b->d_stats, work);
         k_pt_init<TECH, Ctx><<<(unsigned)((L.paths + 127) / 128), 128, 0, s>>>(make<Ctx>(b), st, 0, q);
         PathRayIO<true> io{ st.counters + q, st.qo[q], st.qd[q], st.hit, b->d_table };
-        k_trace_persistent<LAYOUT, STACK, false, PathRayIO<true>><<<L.trace_blocks, 128, 0, s>>>(
-            L.proto, io, b->d_status, work);
+        launch_traversal<LAYOUT, STACK, false>(b, L.trace_blocks, L.proto, io, work, s);
         k_pt_shade<TECH, Ctx><<<L.shade_blocks, 128, 0, s>>>(make<Ctx>(b), st, 0, q, 1 - q);
         if (TECH != LMGPU_RENDER_PT) {
             ShadowIO<FilmCtx> sio{ st.counters + 2, st.sh_o, st.sh_d, st.sh_c, st.L, make<FilmCtx>(b) };
-            k_trace_persistent<LAYOUT, STACK, true, ShadowIO<FilmCtx>><<<L.shadow_blocks, 128, 0, s>>>(
-                L.proto, sio, b->d_status, work + 1);
+            launch_traversal<LAYOUT, STACK, true>(b, L.shadow_blocks, L.proto, sio, work + 1, s);
         }
         k_pt_retire<FilmCtx><<<L.shade_blocks, 128, 0, s>>>(make<FilmCtx>(b), st);
     }
@@ -498,6 +548,7 @@ int run_stream(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_t
     L.shade_blocks = std::max(1, b->cfg.shade_blocks_per_sm) * b->sms;
     L.proto = b->scenes[0]->dev;
     L.proto.layout = LAYOUT;
+    L.proto.stack_cap = STACK;        // every scene of the batch: the largest bound
     S::warm(L);
     const unsigned setup_blocks = (unsigned)std::min<int64_t>((P + 255) / 256, 148 * 16);
     k_stream_setup<<<setup_blocks, 256, 0, s>>>(b->d_ctl, pl.total, P, b->st[0].free_slots, b->st[0].counters, b->d_stats);
@@ -558,6 +609,7 @@ int run_overlap(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_
     L.shade_blocks = std::max(1, b->cfg.shade_blocks_per_sm) * b->sms;
     L.proto = b->scenes[0]->dev;
     L.proto.layout = LAYOUT;
+    L.proto.stack_cap = STACK;        // every scene of the batch: the largest bound
     W::warm(L);
     const int K = pl.bounces;
     const int T = std::min(b->cfg.overlap_bounce > 0 ? b->cfg.overlap_bounce : DEFAULT_OVERLAP_BOUNCE, K + 1);
@@ -640,6 +692,7 @@ int run_waves(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_t&
     L.shade_blocks = std::max(1, b->cfg.shade_blocks_per_sm) * b->sms;
     L.proto = b->scenes[0]->dev;
     L.proto.layout = LAYOUT;
+    L.proto.stack_cap = STACK;        // every scene of the batch: the largest bound
     W::warm(L);
     waves = (pl.total + P - 1) / P;
     k_batch_setup<<<1, 1, 0, s>>>(b->d_wave, 1, pl.total, P, b->d_stats);
@@ -851,6 +904,9 @@ int lmgpu_batch_destroy(LmgpuBatch* b)
     cudaFreeHost(b->h_begins);
     cudaFreeHost(b->h_stats);
     cudaFreeHost(b->h_counts);
+    cudaFree(b->hf_film);
+    cudaFree(b->hf_out);
+    cudaFreeHost(b->hf_pinned);
     delete b;
     return LMGPU_OK;
 }
@@ -877,6 +933,114 @@ int lmgpu_batch_render_device(LmgpuBatch* b, const LmgpuRenderParams* params, vo
 {
     if (!b || !params || !films) return fail(LMGPU_ERR_INVALID, "null argument");
     return batch_render(b, params, films, static_cast<cudaStream_t>(stream), stats);
+}
+
+int lmgpu_batch_render(LmgpuBatch* b, const LmgpuRenderParams* params, float* const* films_host,
+                       LmgpuRenderStats* stats)
+{
+    if (!b || !params || !films_host) return fail(LMGPU_ERR_INVALID, "null argument");
+    const size_t n = b->scenes.size();
+    std::vector<int64_t> off(n + 1, 0);
+    for (size_t i = 0; i < n; i++) {
+        if (!films_host[i]) return fail(LMGPU_ERR_INVALID, "null film");
+        const DeviceScene& d = b->scenes[i]->dev;
+        off[i + 1] = off[i] + 3 * (int64_t)d.cam.width * d.cam.height;
+    }
+    const size_t esize = params[0].film_fp64 ? sizeof(double) : sizeof(float);
+    const size_t film_bytes = (size_t)off[n] * esize, out_bytes = (size_t)off[n] * sizeof(float);
+    if (b->hf_film_bytes < film_bytes) {
+        cudaFree(b->hf_film);
+        b->hf_film = nullptr;
+        b->hf_film_bytes = 0;
+        LMGPU_CUDA_TRY(cudaMalloc(&b->hf_film, film_bytes));
+        b->hf_film_bytes = film_bytes;
+    }
+    if (b->hf_out_bytes < out_bytes) {
+        cudaFree(b->hf_out);
+        cudaFreeHost(b->hf_pinned);
+        b->hf_out = nullptr;
+        b->hf_pinned = nullptr;
+        b->hf_out_bytes = 0;
+        cudaError_t e = cudaMalloc(&b->hf_out, out_bytes);
+        if (e == cudaSuccess) e = cudaMallocHost(&b->hf_pinned, out_bytes);
+        if (e != cudaSuccess) {
+            cudaFree(b->hf_out);
+            b->hf_out = nullptr;
+            b->hf_pinned = nullptr;
+            return cuda_fail(e, "batch film buffers");
+        }
+        b->hf_out_bytes = out_bytes;
+    }
+    std::vector<void*> films(n);
+    for (size_t i = 0; i < n; i++) films[i] = static_cast<char*>(b->hf_film) + (size_t)off[i] * esize;
+    LMGPU_CUDA_TRY(cudaMemsetAsync(b->hf_film, 0, film_bytes, nullptr));
+    LmgpuRenderStats local;
+    int rc = batch_render(b, params, films.data(), nullptr, stats ? stats : &local);
+    if (rc != LMGPU_OK) return rc;
+    // Rescale(W * H / num_samples) per scene (sched.mt.cpp:250-256).
+    for (size_t i = 0; i < n; i++) {
+        const DeviceScene& d = b->scenes[i]->dev;
+        const int64_t m = off[i + 1] - off[i];
+        const double scale = double(d.cam.width) * d.cam.height / double(params[i].num_samples);
+        const unsigned blocks = (unsigned)((m + 255) / 256);
+        if (esize == sizeof(double))
+            k_rescale_film<double><<<blocks, 256>>>(static_cast<const double*>(films[i]), b->hf_out + off[i], m, scale);
+        else
+            k_rescale_film<float><<<blocks, 256>>>(static_cast<const float*>(films[i]), b->hf_out + off[i], m, scale);
+        LMGPU_CUDA_TRY(cudaGetLastError());
+    }
+    LMGPU_CUDA_TRY(cudaMemcpyAsync(b->hf_pinned, b->hf_out, out_bytes, cudaMemcpyDeviceToHost, nullptr));
+    LMGPU_CUDA_TRY(cudaStreamSynchronize(nullptr));
+    for (size_t i = 0; i < n; i++)
+        std::memcpy(films_host[i], b->hf_pinned + off[i], (size_t)(off[i + 1] - off[i]) * sizeof(float));
+    return LMGPU_OK;
+}
+
+int lmgpu_batch_profile(LmgpuBatch* b, const LmgpuRenderParams* params, void* const* films, void* stream,
+                        int32_t count_tests, LmgpuTraceProfile* out)
+{
+    if (!b || !params || !films || !out) return fail(LMGPU_ERR_INVALID, "null argument");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    TraceProfileRun run;
+    run.count = count_tests != 0;
+    if (run.count) {
+        LMGPU_CUDA_TRY(cudaMalloc(&run.d_counts, 4 * sizeof(unsigned long long)));
+        cudaError_t e = cudaMemsetAsync(run.d_counts, 0, 4 * sizeof(unsigned long long), s);
+        if (e != cudaSuccess) { cudaFree(run.d_counts); return cuda_fail(e, "profile counters"); }
+    }
+    const LmgpuBatchConfig saved = b->cfg;
+    b->cfg.use_graph = 0;
+    b->cfg.mode = LMGPU_BATCH_WAVES;
+    b->prof = &run;
+    LmgpuRenderStats st;
+    std::memset(&st, 0, sizeof(st));
+    int rc = batch_render(b, params, films, s, &st);
+    b->prof = nullptr;
+    b->cfg = saved;
+    if (rc == LMGPU_OK && run.error != cudaSuccess) rc = cuda_fail(run.error, "profile events");
+    std::memset(out, 0, sizeof(*out));
+    out->rays[0] = st.rays_traced - st.shadow_rays;
+    out->rays[1] = st.shadow_rays;
+    out->render_ms = st.device_ms;
+    for (size_t k = 0; k < run.kinds.size() && rc == LMGPU_OK; k++) {
+        float ms = 0.0f;
+        const cudaError_t e = cudaEventElapsedTime(&ms, run.events[2 * k], run.events[2 * k + 1]);
+        if (e != cudaSuccess) { rc = cuda_fail(e, "profile event times"); break; }
+        out->trace_ms[run.kinds[k]] += ms;
+        out->launches[run.kinds[k]]++;
+    }
+    for (cudaEvent_t e : run.events) cudaEventDestroy(e);
+    if (run.count) {
+        unsigned long long h[4] = {};
+        if (rc == LMGPU_OK) {
+            const cudaError_t e = cudaMemcpy(h, run.d_counts, sizeof(h), cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) rc = cuda_fail(e, "profile counters");
+        }
+        out->node_tests[0] = h[0]; out->tri_tests[0] = h[1];
+        out->node_tests[1] = h[2]; out->tri_tests[1] = h[3];
+        cudaFree(run.d_counts);
+    }
+    return rc;
 }
 
 int lmgpu_batch_autotune(LmgpuBatch* b, const LmgpuRenderParams* params, double fraction, void* stream,

@@ -34,9 +34,9 @@ __device__ __forceinline__ bool trace_scene(const DeviceScene& s, TraversalRay& 
 {
     if (s.num_tris == 0) { h.tri = -1; return true; }   // empty scene: no node arrays exist
     if (LAYOUT == LMGPU_LAYOUT_BVH2)
-        return trace_bvh2<ANY_HIT>(s.bvh2, s.tris, s.root_ref, s.root_box, r, h, stack, STACK, nullptr);
+        return trace_bvh2<ANY_HIT>(s.bvh2, s.tris, s.root_ref, s.root_box, r, h, stack, s.stack_cap < STACK ? s.stack_cap : STACK, nullptr);
     if (LAYOUT == LMGPU_LAYOUT_BVH4)
-        return trace_bvh4<ANY_HIT>(s.bvh4, s.tris, s.root_ref4, s.root_box, r, h, stack, STACK, nullptr);
+        return trace_bvh4<ANY_HIT>(s.bvh4, s.tris, s.root_ref4, s.root_box, r, h, stack, s.stack_cap < STACK ? s.stack_cap : STACK, nullptr);
     trace_naive<ANY_HIT>(s.tris_by_id, s.num_tris, r, h, nullptr);
     return true;
 }

@@ -77,10 +77,22 @@ struct LaneScene {
 
 template <int LAYOUT, int EXIT, class Stack>
 __device__ __forceinline__ bool descend(const LaneScene& s, TravState& ts, Stack stack, int cap,
-                                        const TraversalRay& r, bool may_exit)
+                                        const TraversalRay& r, bool may_exit, TraceStats* st)
 {
-    if (LAYOUT == LMGPU_LAYOUT_BVH2) return bvh2_descend<EXIT>(s.bvh2, ts, stack, cap, r, nullptr, may_exit);
-    return bvh4_descend<EXIT>(s.bvh4, ts, stack, cap, r, nullptr, may_exit);
+    if (LAYOUT == LMGPU_LAYOUT_BVH2) return bvh2_descend<EXIT>(s.bvh2, ts, stack, cap, r, st, may_exit);
+    return bvh4_descend<EXIT>(s.bvh4, ts, stack, cap, r, st, may_exit);
+}
+
+// Adds each lane's counts to counts[0] (binary-node slab tests; four per
+// 4-wide node) and counts[1] (TriAccel tests); the whole warp calls it.
+__device__ __forceinline__ void add_trace_stats(const TraceStats& st, unsigned long long* counts)
+{
+    unsigned long long a = st.nodes, b = st.tris;
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    if ((threadIdx.x & 31u) == 0) { atomicAdd(counts, a); atomicAdd(counts + 1, b); }
 }
 
 // Persistent traversal with per-lane ray replacement: a warp keeps tracing
@@ -96,9 +108,13 @@ __device__ __forceinline__ bool descend(const LaneScene& s, TravState& ts, Stack
 // 2^24-ray soup this raised the kernel from 1.48 to 2.29 Grays/s).
 // For a multi-scene I/O policy each lane switches to its new ray's scene at
 // refill (node and triangle arrays, root); an empty scene is a miss.
-template <int LAYOUT, int STACK, bool ANY_HIT, class IO>
+// The COUNT instantiation (measurement runs only) also adds the rays' slab
+// and TriAccel tests to counts[0..1]; the walk is the same. The stack bound
+// is the scene's stack_cap where that is below STACK.
+template <int LAYOUT, int STACK, bool ANY_HIT, class IO, bool COUNT = false>
 __global__ void __launch_bounds__(128, min_blocks<IO>::value)
-k_trace_persistent(const DeviceScene s, const IO io, int32_t* status, unsigned long long* next_ray)
+k_trace_persistent(const DeviceScene s, const IO io, int32_t* status, unsigned long long* next_ray,
+                   unsigned long long* counts)
 {
     constexpr unsigned FULL = 0xffffffffu;
 #if LMGPU_TRACE_SHARED_STACK > 0
@@ -112,7 +128,10 @@ k_trace_persistent(const DeviceScene s, const IO io, int32_t* status, unsigned l
     const int64_t n = io.count();
     const unsigned lane = threadIdx.x & 31u;
     const int32_t root = LAYOUT == LMGPU_LAYOUT_BVH2 ? s.root_ref : s.root_ref4;
+    const int cap = s.stack_cap < STACK ? s.stack_cap : STACK;
     LaneScene ls{ s.bvh2, s.bvh4, s.tris };
+    TraceStats stats{ 0, 0 };
+    TraceStats* const st = COUNT ? &stats : nullptr;
     TraversalRay r;
     Hit h;
     h.tri = -1;
@@ -141,9 +160,9 @@ k_trace_persistent(const DeviceScene s, const IO io, int32_t* status, unsigned l
                         ls.bvh4 = rs.bvh4;
                         ls.tris = rs.tris;
                         if (rs.num_tris > 0)
-                            trav_begin(ts, LAYOUT == LMGPU_LAYOUT_BVH2 ? rs.root_ref : rs.root_ref4, rs.root_box, r, nullptr);
+                            trav_begin(ts, LAYOUT == LMGPU_LAYOUT_BVH2 ? rs.root_ref : rs.root_ref4, rs.root_box, r, st);
                     } else {
-                        trav_begin(ts, root, s.root_box, r, nullptr);
+                        trav_begin(ts, root, s.root_box, r, st);
                     }
                     if (ts.ref == REF_DONE) io.store(idx, h, r);
                 }
@@ -152,17 +171,20 @@ k_trace_persistent(const DeviceScene s, const IO io, int32_t* status, unsigned l
             break;
         }
         if (ts.ref != REF_DONE) {
-            if (!descend<LAYOUT, exit_below<IO>::value>(ls, ts, stack, STACK, r, !exhausted)) {
+            if (!descend<LAYOUT, exit_below<IO>::value>(ls, ts, stack, cap, r, !exhausted, st)) {
                 atomicOr(status, STATUS_STACK_OVERFLOW);
                 h.tri = -1;
                 ts.ref = REF_DONE;
             } else if (ts.ref < 0) {           // at a leaf (a paused descent resumes next round)
-                if (trace_leaf<ANY_HIT>(ls.tris, ~ts.ref, r, h, nullptr) && ANY_HIT) ts.ref = REF_DONE;
-                else pop_next(ts, stack, r, nullptr);
+                // (a binary pop is the reference's far-child test; 4-wide
+                // nodes count their four slab tests when fetched)
+                if (trace_leaf<ANY_HIT>(ls.tris, ~ts.ref, r, h, st) && ANY_HIT) ts.ref = REF_DONE;
+                else pop_next(ts, stack, r, LAYOUT == LMGPU_LAYOUT_BVH2 ? st : nullptr);
             }
             if (ts.ref == REF_DONE) io.store(idx, h, r);
         }
     }
+    if (COUNT) add_trace_stats(stats, counts);
 }
 
 // Brute-force traversal for the naive layout (one thread per ray).
@@ -190,12 +212,15 @@ int resident_blocks(K kernel)
 
 // Launches the traversal for `io` on `stream`: persistent kernel for the
 // BVH layouts (with the scene's work counter reset first), brute force for
-// the naive layout. `max_rays` bounds the grid (0 = resident grid).
-template <bool ANY_HIT, int STACK, class IO>
-int launch_trace_stack(LmgpuScene* sc, const IO& io, int64_t max_rays, cudaStream_t stream)
+// the naive layout. `max_rays` bounds the grid (0 = resident grid). COUNT
+// launches the counting instantiation, adding to `counts` (BVH layouts).
+template <bool ANY_HIT, int STACK, bool COUNT, class IO>
+int launch_trace_stack(LmgpuScene* sc, const IO& io, int64_t max_rays, cudaStream_t stream,
+                       unsigned long long* counts)
 {
     const DeviceScene& s = sc->dev;
     if (s.layout == LMGPU_LAYOUT_NAIVE || s.num_tris == 0) {
+        if (COUNT) return fail(LMGPU_ERR_UNSUPPORTED, "traversal counters need a BVH layout");
         const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((max_rays + 127) / 128, 148 * 64));
         k_trace_naive<ANY_HIT, IO><<<blocks, 128, 0, stream>>>(s, io);
         LMGPU_CUDA_TRY(cudaGetLastError());
@@ -206,28 +231,29 @@ int launch_trace_stack(LmgpuScene* sc, const IO& io, int64_t max_rays, cudaStrea
     unsigned long long* work = sc->d_work + (sc->work_slot++ % LmgpuScene::WORK_SLOTS);
     LMGPU_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(unsigned long long), stream));
     if (s.layout == LMGPU_LAYOUT_BVH2) {
-        auto k = k_trace_persistent<LMGPU_LAYOUT_BVH2, STACK, ANY_HIT, IO>;
+        auto k = k_trace_persistent<LMGPU_LAYOUT_BVH2, STACK, ANY_HIT, IO, COUNT>;
         int64_t blocks = resident_blocks(k);
         if (max_rays > 0) blocks = std::max<int64_t>(1, std::min<int64_t>(blocks, (max_rays + 127) / 128));
-        k<<<blocks, 128, 0, stream>>>(s, io, sc->d_status, work);
+        k<<<blocks, 128, 0, stream>>>(s, io, sc->d_status, work, counts);
     } else {
-        auto k = k_trace_persistent<LMGPU_LAYOUT_BVH4, STACK, ANY_HIT, IO>;
+        auto k = k_trace_persistent<LMGPU_LAYOUT_BVH4, STACK, ANY_HIT, IO, COUNT>;
         int64_t blocks = resident_blocks(k);
         if (max_rays > 0) blocks = std::max<int64_t>(1, std::min<int64_t>(blocks, (max_rays + 127) / 128));
-        k<<<blocks, 128, 0, stream>>>(s, io, sc->d_status, work);
+        k<<<blocks, 128, 0, stream>>>(s, io, sc->d_status, work, counts);
     }
     LMGPU_CUDA_TRY(cudaGetLastError());
     return LMGPU_OK;
 }
 
-template <bool ANY_HIT, class IO>
-int launch_trace(LmgpuScene* sc, const IO& io, int64_t max_rays, cudaStream_t stream)
+template <bool ANY_HIT, class IO, bool COUNT = false>
+int launch_trace(LmgpuScene* sc, const IO& io, int64_t max_rays, cudaStream_t stream,
+                 unsigned long long* counts = nullptr)
 {
     const int cap = sc->dev.stack_cap;
-    if (cap <= 32) return launch_trace_stack<ANY_HIT, 32>(sc, io, max_rays, stream);
-    if (cap <= 64) return launch_trace_stack<ANY_HIT, 64>(sc, io, max_rays, stream);
-    if (cap <= 128) return launch_trace_stack<ANY_HIT, 128>(sc, io, max_rays, stream);
-    if (cap <= 256) return launch_trace_stack<ANY_HIT, 256>(sc, io, max_rays, stream);
+    if (cap <= 32) return launch_trace_stack<ANY_HIT, 32, COUNT>(sc, io, max_rays, stream, counts);
+    if (cap <= 64) return launch_trace_stack<ANY_HIT, 64, COUNT>(sc, io, max_rays, stream, counts);
+    if (cap <= 128) return launch_trace_stack<ANY_HIT, 128, COUNT>(sc, io, max_rays, stream, counts);
+    if (cap <= 256) return launch_trace_stack<ANY_HIT, 256, COUNT>(sc, io, max_rays, stream, counts);
     return fail(LMGPU_ERR_UNSUPPORTED, "BVH deeper than the largest compiled traversal stack (256)");
 }
 

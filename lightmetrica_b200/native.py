@@ -63,7 +63,7 @@ class SceneDesc(ctypes.Structure):
                 ("has_camera", c_int32), ("camera_eye", c_float * 3), ("camera_center", c_float * 3),
                 ("camera_up", c_float * 3), ("camera_fovy_degrees", c_float),
                 ("film_width", c_int32), ("film_height", c_int32),
-                ("layout", c_int32), ("build_threads", c_int32)]
+                ("layout", c_int32), ("build_threads", c_int32), ("max_stack_entries", c_int32)]
 
 
 class SceneInfo(ctypes.Structure):
@@ -104,6 +104,11 @@ class BatchConfig(ctypes.Structure):
                 ("use_graph", c_int32), ("mode", c_int32), ("overlap_bounce", c_int32)]
 
 
+class TraceProfile(ctypes.Structure):
+    _fields_ = [("rays", c_int64 * 2), ("launches", c_int64 * 2), ("trace_ms", c_double * 2),
+                ("render_ms", c_double), ("node_tests", c_uint64 * 2), ("tri_tests", c_uint64 * 2)]
+
+
 # Every symbol include/lmgpu.h declares, with (restype, argtypes).
 SIGNATURES = {
     "lmgpu_abi_version": (c_int32, []),
@@ -132,6 +137,8 @@ SIGNATURES = {
     "lmgpu_batch_render_device": (c_int32, [c_void_p, P(RenderParams), P(c_void_p), c_void_p, P(RenderStats)]),
     "lmgpu_batch_autotune": (c_int32, [c_void_p, P(RenderParams), c_double, c_void_p, P(BatchConfig),
                                        P(c_double)]),
+    "lmgpu_batch_render": (c_int32, [c_void_p, P(RenderParams), P(c_void_p), P(RenderStats)]),
+    "lmgpu_batch_profile": (c_int32, [c_void_p, P(RenderParams), P(c_void_p), c_void_p, c_int32, P(TraceProfile)]),
     "lmgpu_eval_sampling": (c_int32, [c_int32, c_void_p, c_int64, c_void_p]),
     "lmgpu_camera_sample_rays": (c_int32, [c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
     "lmgpu_camera_raster_positions": (c_int32, [c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),

@@ -198,6 +198,7 @@ class Scene:
         self.layout = _LAYOUTS[impl]
         self.primitives: Optional[Primitives] = None
         self.build_threads = 0
+        self.max_stack_entries = 0
         self.handle = None
         self._keep = []
 
@@ -205,10 +206,14 @@ class Scene:
     def load(self, primitives: Primitives) -> None:
         self.primitives = primitives
 
-    # reference Scene::Configure: the GPU scene reads `build_threads`.
+    # reference Scene::Configure: the GPU scene reads `build_threads` and
+    # `max_stack_entries` (the traversal stack bound per ray, 0 = automatic).
     def configure(self, node: Optional[dict] = None) -> bool:
         node = node or {}
         self.build_threads = int(node.get("build_threads", 0))
+        self.max_stack_entries = int(node.get("max_stack_entries", 0))
+        if self.max_stack_entries < 0:
+            raise ValueError("max_stack_entries must be >= 0")
         return True
 
     def build(self) -> bool:
@@ -363,6 +368,7 @@ class Scene:
             desc.film_height = cam.film.height
         desc.layout = self.layout
         desc.build_threads = self.build_threads
+        desc.max_stack_entries = self.max_stack_entries
         keep += [prims, mat_arr, light_arr]
         return desc, keep
 

@@ -285,18 +285,10 @@ def flatten_primitives(prims):
     return out
 
 
-def ref_render(prims, renderer="pt", num_samples=None, spp=16, rr_depth=1, max_path_vertices=-1, seed=1,
-               threads=None, precision="d", samples_per_block=100, scene_type="bvh", sched_type="mt"):
-    """Renders `prims` with the reference's own component wiring (oracle/_ref):
-    renderer `renderer`, scheduler `sched_type` (the reference's "mt") and
-    accelerator `scene_type` (the reference's "bvh"); a loaded plugin's
-    components ("plugin.gpu", "gpu.pt.mis", "gpu") can take any of the three
-    slots. Returns (film (H, W, 3) float32, render seconds)."""
-    L = ref(precision)
-    if not hasattr(L, "lmref_render"):
-        raise RuntimeError("reference harness built without the renderer")
-    L.lmref_render.restype = ctypes.c_double
-    L.lmref_render.argtypes = [ctypes.POINTER(_RefRenderDesc), ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+def _ref_desc(prims, renderer, num_samples, spp, rr_depth, max_path_vertices, seed, threads, samples_per_block,
+              scene_type, sched_type):
+    """The harness's flat scene description of `prims`, with the arrays it
+    points into (keep them alive while the description is in use)."""
     fl = flatten_primitives(prims)
     cam = prims.camera
     W, H = cam.film.width, cam.film.height
@@ -307,6 +299,7 @@ def ref_render(prims, renderer="pt", num_samples=None, spp=16, rr_depth=1, max_p
         a = (ctypes.c_void_p * n)(*[x.ctypes.data for x in arrs])
         keep.append(a)
         return a
+    keep += [fl]
     nv = np.array([x.size // 3 for x in fl["pos"]], np.int32)
     nf = np.array([x.size // 3 for x in fl["faces"]], np.int32)
     mat = np.array(fl["mat"], np.int32)
@@ -343,13 +336,91 @@ def ref_render(prims, renderer="pt", num_samples=None, spp=16, rr_depth=1, max_p
     d.samples_per_block = samples_per_block
     d.scene_type = scene_type.encode()
     d.sched_type = sched_type.encode()
-    film = np.zeros((H, W, 3), np.float32)
+    keep += [d.renderer, d.scene_type, d.sched_type]
+    return d, keep
+
+
+def _ref_error(L, code):
+    L.lmref_last_error.restype = ctypes.c_char_p
+    return f"reference render failed ({code}): {L.lmref_last_error().decode(errors='replace')}"
+
+
+def ref_render(prims, renderer="pt", num_samples=None, spp=16, rr_depth=1, max_path_vertices=-1, seed=1,
+               threads=None, precision="d", samples_per_block=100, scene_type="bvh", sched_type="mt"):
+    """Renders `prims` with the reference's own component wiring (oracle/_ref):
+    renderer `renderer`, scheduler `sched_type` (the reference's "mt") and
+    accelerator `scene_type` (the reference's "bvh"); a loaded plugin's
+    components ("plugin.gpu", "gpu.pt.mis", "gpu") can take any of the three
+    slots. Returns (film (H, W, 3) float32, render seconds)."""
+    L = ref(precision)
+    if not hasattr(L, "lmref_render"):
+        raise RuntimeError("reference harness built without the renderer")
+    L.lmref_render.restype = ctypes.c_double
+    L.lmref_render.argtypes = [ctypes.POINTER(_RefRenderDesc), ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+    d, keep = _ref_desc(prims, renderer, num_samples, spp, rr_depth, max_path_vertices, seed, threads,
+                        samples_per_block, scene_type, sched_type)
+    cam = prims.camera
+    film = np.zeros((cam.film.height, cam.film.width, 3), np.float32)
     bt = ctypes.c_double()
     secs = L.lmref_render(ctypes.byref(d), film.ctypes.data, ctypes.byref(bt))
+    del keep
     if secs < 0:
-        L.lmref_last_error.restype = ctypes.c_char_p
-        raise RuntimeError(f"reference render failed ({secs}): {L.lmref_last_error().decode(errors='replace')}")
+        raise RuntimeError(_ref_error(L, secs))
     return film, secs
+
+
+class RefRenderSession:
+    """The reference's renderer (oracle/_ref, its own `mt` scheduler and
+    `bvh` scene) built once and rendered several times: the timed CPU
+    baseline of the path tracer. The scene is wrapped in the harness's
+    counting scene, so every render reports the rays it traced (camera,
+    bounce and shadow rays: every Scene::Intersect, scene.cpp:67-72).
+    Successive renders continue the renderer's sampler (fresh samples)."""
+
+    def __init__(self, prims, renderer="pt.mis", rr_depth=1, max_path_vertices=-1, seed=1, precision="f",
+                 samples_per_block=100):
+        L = ref(precision)
+        if not hasattr(L, "lmref_session_create"):
+            raise RuntimeError("reference harness built without render sessions")
+        L.lmref_session_create.restype = ctypes.c_void_p
+        L.lmref_session_create.argtypes = [ctypes.POINTER(_RefRenderDesc), ctypes.POINTER(ctypes.c_double),
+                                           ctypes.POINTER(ctypes.c_int)]
+        L.lmref_session_render.restype = ctypes.c_double
+        L.lmref_session_render.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int, ctypes.c_void_p,
+                                           ctypes.POINTER(ctypes.c_longlong)]
+        L.lmref_session_destroy.argtypes = [ctypes.c_void_p]
+        self._L = L
+        d, keep = _ref_desc(prims, renderer, 1, 1, rr_depth, max_path_vertices, seed, None, samples_per_block,
+                            "harness.counting", "mt")
+        bt, st = ctypes.c_double(), ctypes.c_int()
+        self._h = L.lmref_session_create(ctypes.byref(d), ctypes.byref(bt), ctypes.byref(st))
+        del keep
+        if not self._h:
+            raise RuntimeError(_ref_error(L, st.value))
+        self.build_seconds = bt.value
+        self.width, self.height = prims.camera.film.width, prims.camera.film.height
+
+    def render(self, num_samples: int, threads=None, film: bool = False):
+        """Renders `num_samples` samples; returns (seconds of sched.Render,
+        rays traced, rescaled film (H, W, 3) or None)."""
+        out = np.zeros((self.height, self.width, 3), np.float32) if film else None
+        rays = ctypes.c_longlong()
+        secs = self._L.lmref_session_render(self._h, int(num_samples), int(threads or os.cpu_count() or 1),
+                                            None if out is None else out.ctypes.data, ctypes.byref(rays))
+        if secs < 0:
+            raise RuntimeError(_ref_error(self._L, secs))
+        return secs, rays.value, out
+
+    def close(self):
+        if self._h:
+            self._L.lmref_session_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class _OrcPtDesc(ctypes.Structure):

@@ -21,6 +21,9 @@ Fixtures:
                            the reference's double-precision pt.mis image of
                            lightmetrica_b200.scenes.cornell_box(128, 128,
                            variant) (4096 / 16384 spp)
+  cornell_c1_256_ref_mis.npz
+                           the reference's double-precision pt.mis image of
+                           scenes.cornell_box(256, 256) at max depth 8 (4096 spp)
   terrain_ref_mis_96x54.npz
                            the reference's double-precision pt.mis image of
                            scenes.terrain_spheres at 96 x 54 (16384 spp)
@@ -157,6 +160,20 @@ def images(variants=("classic", "mixed")):
         print("wrote", variant, "image", f"{spp} spp {secs:.1f} s", film.mean(axis=(0, 1)))
 
 
+def c1_image(spp: int = 4096):
+    """Image oracle of the plain path-tracer configuration: the Cornell box
+    (scenes.cornell_box "classic": 10 wall, 24 box and 2 light triangles,
+    Le (17, 12, 4)) at exactly 256 x 256, 40 degree field of view, max depth
+    8 (max_path_vertices 9), Russian roulette from vertex 3 (rr_depth 3),
+    seed 1: the reference's double-precision pt.mis at 4096 spp."""
+    from lightmetrica_b200 import scenes
+    prims = scenes.cornell_box(256, 256, variant="classic")
+    film, secs = oracle.ref_render(prims, "pt.mis", spp=spp, rr_depth=3, max_path_vertices=9, seed=1)
+    np.savez_compressed(os.path.join(OUT, "cornell_c1_256_ref_mis.npz"), film=film, spp=spp, rr_depth=3,
+                        max_path_vertices=9, seconds=secs)
+    print("wrote C1 image", f"{spp} spp {secs:.1f} s", film.mean(axis=(0, 1)))
+
+
 def terrain_image(spp: int = 16384):
     """Image oracle of the full path-tracer scene (scenes.terrain_spheres: a
     1024 x 1024-vertex fBm heightfield, 64 level-5 icospheres, a spherical
@@ -202,4 +219,5 @@ if __name__ == "__main__":
     scene_literals()
     if oracle.ref_available("d"):
         images()
+        c1_image()
         terrain_image()

@@ -217,3 +217,58 @@ def test_batch_errors(cuda):
     with pytest.raises(ValueError):
         batch.configure(layout="naive")
     batch.close()
+
+
+def test_batch_profile_counts_and_times(cuda):
+    """lmgpu_batch_profile: the counting and the timed measurement renders
+    trace the same paths as a plain render (films equal the one-scene
+    renderer's), and report per-kind rays, launches, device times and the
+    traversal work counts."""
+    import torch
+    items = small_set()
+    built = [build(p) for p, _, _ in items]
+    want = plain_films(built, items)
+    batch = SceneBatch(built)
+    rs, ns = [r for _, r, _ in items], [n for _, _, n in items]
+    films = [torch.zeros(p.camera.film.width * p.camera.film.height * 3, dtype=torch.float64, device="cuda")
+             for p, _, _ in items]
+    counted = batch.profile(rs, ns, films, count_tests=True)
+    assert_same([f.cpu().numpy() for f in films], want)
+    for f in films:
+        f.zero_()
+    timed = batch.profile(rs, ns, films, count_tests=False)
+    assert_same([f.cpu().numpy() for f in films], want)
+    batch.render_device(rs, ns, films)
+    st = batch.last_stats
+    for k in ("closest", "shadow"):
+        c, t = counted[k], timed[k]
+        assert c["rays"] == t["rays"] > 0 and c["launches"] == t["launches"] > 0
+        assert t["trace_ms"] > 0
+        # Every ray tests at least the root box; the scenes are hit often.
+        assert c["node_tests"] >= c["rays"] and c["tri_tests"] > 0
+    assert counted["closest"]["rays"] + counted["shadow"]["rays"] == st["rays_traced"]
+    assert counted["shadow"]["rays"] == st["shadow_rays"]
+    assert timed["render_ms"] > timed["closest"]["trace_ms"] + timed["shadow"]["trace_ms"]
+    batch.close()
+
+
+def test_batch_films_match_reference_goldens(cuda, golden_dir):
+    """The golden Cornell scenes rendered inside a batch together with other
+    scenes: each of their films against the reference's double-precision
+    pt.mis image (relMSE <= 1e-3, the bar of the one-scene image tests)."""
+    import os
+    ref = {v: np.load(os.path.join(golden_dir, f"cornell_{v}_ref_mis.npz"))["film"] for v in ("classic", "mixed")}
+    spp = 16384
+    items = [(scenes.cornell_box(128, 128, variant="classic"), renderer("pt.mis", 3, 9, 7), 128 * 128 * spp),
+             (scenes.cornell_box(128, 128, variant="mixed"), renderer("pt.mis", 3, 9, 8), 128 * 128 * spp)]
+    items += small_set()[2:4]
+    built = [build(p) for p, _, _ in items]
+    batch = SceneBatch(built)
+    films = batch.render([r for _, r, _ in items], [n for _, _, n in items])
+    for variant, f in zip(("classic", "mixed"), films[:2]):
+        e = float(np.mean((f - ref[variant]) ** 2 / (ref[variant] ** 2 + 1e-2)))
+        print(f"batch {variant}: relMSE {e:.3e}")
+        assert np.isfinite(f).all() and e <= 1e-3
+    for f in films[2:]:
+        assert np.isfinite(f).all() and f.max() > 0
+    batch.close()

@@ -243,3 +243,85 @@ def test_host_pipeline_pinned_and_pageable_buffers(cuda, pinned_in, pinned_out):
     for o, k in zip(outs[1:], ("t", "u", "v")):
         np.testing.assert_array_equal(o.numpy(), want[k])
 
+
+
+@pytest.mark.skipif(not oracle.ref_available("f"), reason="reference harness (oracle/_ref) not built")
+def test_full_benchmark_batch_bit_exact_vs_reference(cuda):
+    """All 2^24 rays of the intersection benchmark against the reference's
+    own BVHScene (oracle/_ref, its float build, on all host threads): ids
+    bit-exact and hit distances bit-equal, for the binary layout and its
+    4-wide collapse."""
+    pos, faces = random_soup(1 << 20, seed=1)
+    rays = random_rays(1 << 24, seed=2)
+    want = oracle.RefScene(pos, faces, "bvh").intersect(rays, threads=os.cpu_count() or 1)
+    hit = want["tri_id"] >= 0
+    assert 0.15 < hit.mean() < 0.35
+    for layout in LAYOUTS:
+        got = gpu_scene(pos, faces, layout).intersect_host(rays)
+        np.testing.assert_array_equal(got["tri_id"], want["tri_id"])
+        np.testing.assert_array_equal(got["t"][hit], want["t"][hit])
+
+
+def test_stack_bound_overflow_is_reported_and_recoverable(cuda):
+    """A scene whose traversal stack bound (max_stack_entries) is below what
+    its walks need: the kernels flag the overflow in the scene's status word
+    and return (no trap), the call reports LMGPU_ERR_STACK_OVERFLOW, and the
+    status is cleared: the next call on the same scene succeeds when its rays
+    need no stack, and the same rays succeed on a scene with the automatic
+    bound."""
+    import torch
+    pos, faces = random_soup(50000, seed=71, sigma=0.05)
+    rays = random_rays(20000, seed=72)
+    for layout in LAYOUTS:
+        s = Scene(layout)
+        s.load(soup_primitives(pos, faces))
+        s.configure({"max_stack_entries": 2})
+        s.build()
+        with pytest.raises(native.LmgpuError) as e:
+            s.intersect_host(rays)
+        assert e.value.code == native.ERR_STACK_OVERFLOW
+        # Device entry point: the status word carries it to lmgpu_scene_status.
+        soa = {k: torch.from_numpy(v).to(cuda) for k, v in rays_soa(rays).items()}
+        out = torch.empty(rays.shape[0], dtype=torch.int32, device=cuda)
+        stream = torch.cuda.current_stream().cuda_stream
+        s.intersect_device({k: soa[k].data_ptr() for k in soa}, {"tri_id": out.data_ptr()}, rays.shape[0], stream)
+        with pytest.raises(native.LmgpuError) as e:
+            s.status(stream)
+        assert e.value.code == native.ERR_STACK_OVERFLOW
+        s.status(stream)                              # cleared
+        # Rays that miss the root box need no stack: the next call succeeds.
+        away = rays.copy()
+        away[:, 0:3] = 10.0
+        away[:, 3:6] = np.array([1.0, 0.0, 0.0], np.float32)
+        r = s.intersect_host(away)
+        assert (r["tri_id"] == -1).all()
+        ok = gpu_scene(pos, faces, layout).intersect_host(rays)
+        o = oracle.OracleScene(pos, faces, "bvh").intersect(rays)
+        np.testing.assert_array_equal(ok["tri_id"], o["tri_id"])
+        s.close()
+
+
+def test_stack_bound_overflow_in_a_render(cuda):
+    """The same bound in the path tracer: the render's traversal kernels flag
+    the overflow and lmgpu_render reports LMGPU_ERR_STACK_OVERFLOW; a render
+    of the scene with the automatic bound then succeeds."""
+    from lightmetrica_b200 import create_renderer, create_scheduler, scenes
+    prims = scenes.cornell_refined(3, 32, 32)
+    r = create_renderer("pt.mis")
+    r.configure({"rr_depth": 3, "max_path_vertices": 6, "sampler": {"rng_seed": 1}})
+    sched = create_scheduler("mt")
+    sched.configure({"num_samples": 32 * 32 * 4})
+    capped = Scene("bvh")
+    capped.load(prims)
+    capped.configure({"max_stack_entries": 1})
+    capped.build()
+    with pytest.raises(native.LmgpuError) as e:
+        sched.render(r, capped)
+    assert e.value.code == native.ERR_STACK_OVERFLOW
+    capped.close()
+    s = Scene("bvh")
+    s.load(prims)
+    s.configure({})
+    s.build()
+    assert sched.render(r, s).max() > 0
+    s.close()
