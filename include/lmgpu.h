@@ -63,6 +63,16 @@ enum {
 
 typedef struct LmgpuScene LmgpuScene;
 
+/* The tree the path tracer traverses (LmgpuSceneDesc.render_tree). The
+ * intersection entry points always use the reference's tree, whose closest
+ * hits are bit-exact; renders need only the same expected image, so by
+ * default they trace a second tree built for traversal cost: binned SAH over
+ * all three axes (32 bins), leaves of up to 8 triangles. */
+enum {
+    LMGPU_RENDER_TREE_SAH = 0,        /* a separate render tree (default) */
+    LMGPU_RENDER_TREE_REFERENCE = 1   /* render with the reference's tree */
+};
+
 /* One lightmetrica Primitive (reference include/lightmetrica/primitive.h:39-60)
  * with its TriangleMesh (trianglemesh.h:34-84). Vertices are in object space;
  * `transform` is the primitive's 4x4 matrix, column-major like the
@@ -113,6 +123,7 @@ typedef struct {
                                    need more fail with LMGPU_ERR_STACK_OVERFLOW (the status word
                                    the kernels raise). The multi-scene batch always uses the
                                    largest compiled bound. */
+    int32_t render_tree;        /* LMGPU_RENDER_TREE_* (BVH layouts; 0 = SAH render tree) */
 } LmgpuSceneDesc;
 
 typedef struct {
@@ -125,6 +136,11 @@ typedef struct {
     double build_seconds;       /* host BVH build time */
     float bounds_min[3];        /* Scene::GetAABBTriangles */
     float bounds_max[3];
+    int32_t render_tree;        /* LMGPU_RENDER_TREE_* the renders traverse */
+    int32_t render_max_depth;   /* render tree: depth, nodes, leaves, host build time */
+    int64_t render_num_nodes;
+    int64_t render_num_leaves;
+    double render_build_seconds;
 } LmgpuSceneInfo;
 
 /* Replaces Scene::Load + Configure + Build (reference scene.h:47-191,

@@ -9,16 +9,30 @@
 // dL/dI_p * c / R_t to the gradient of the albedo R of every diffuse vertex t
 // on the contribution's prefix (c is linear in each of them) and
 // dL/dI_p * c / Le to the emission of its light. A path's contributions come
-// in order of non-decreasing prefix length, so the replay keeps, per vertex,
-// the sum of the weights w = dL/dI_p * c whose prefix ends there and turns
-// them into suffix sums once the path is done: one set of atomics per
-// vertex instead of one per (contribution, vertex). Emission gradients are
-// summed per thread and per block before they reach global memory, since
-// every path adds to the same few lights. Russian-roulette
-// probabilities and MIS weights are held at their sampled values, which keeps
-// the estimator unbiased for the diffuse BSDFs (their sampling densities do
-// not depend on R). Per-vertex records live in a fixed local array
-// (MAX_REPLAY_VERTS); longer paths flag LMGPU_ERR_QUEUE_OVERFLOW.
+// in order of non-decreasing prefix length ("depth"), so the replay keeps,
+// for the first RECORDED_VERTS vertices, the sum of the weights
+// w = dL/dI_p * c whose prefix ends there and turns them into suffix sums
+// once the path is done: one set of atomics per vertex instead of one per
+// (contribution, vertex). Emission gradients are summed per thread and per
+// block before they reach global memory, since every path adds to the same
+// few lights. Russian-roulette probabilities and MIS weights are held at
+// their sampled values, which keeps the estimator unbiased for the diffuse
+// BSDFs (their sampling densities do not depend on R).
+//
+// Paths deeper than RECORDED_VERTS vertices: the weights of all
+// contributions deeper than that are summed into one total W_tail while the
+// path runs, and the path's state on arrival at that depth is kept as a
+// checkpoint (position, direction, throughput, previous vertex: a few
+// registers' worth). When the path has ended, the first vertices' suffix
+// sums start from W_tail, and the tail is replayed from the checkpoint a
+// second time: a vertex i there is on the prefix of exactly the tail
+// contributions deeper than i, so its weight is W_tail minus the running sum
+// of the tail contributions met before it; no per-vertex record is needed.
+// Only long paths pay for the second replay of their tail. A replay stops at
+// MAX_PATH_VERTICES surface vertices and flags LMGPU_ERR_QUEUE_OVERFLOW: paths
+// that long occur only in closed scenes without Russian roulette, where the
+// reference's own loop (pathtrace*.cpp, `while (true)` with
+// max_path_vertices = -1) does not end either.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cstring>
@@ -33,7 +47,8 @@
 namespace lmgpu {
 namespace {
 
-constexpr int MAX_REPLAY_VERTS = 64;
+constexpr int RECORDED_VERTS = 32;          // vertices with a per-vertex record
+constexpr int MAX_PATH_VERTICES = 4096;     // replay bound (surface vertices)
 
 struct DiffConsts {
     int32_t technique, rr_depth, max_pv, sampling;
@@ -53,12 +68,16 @@ __device__ __forceinline__ int32_t cast_ray(const DeviceScene& s, V3 o, V3 d, fl
     in.d[0] = d.x; in.d[1] = d.y; in.d[2] = d.z;
     in.tmin = tmin; in.tmax = tmax;
     TraversalRay r;
-    setup_ray(r, in);
+    setup_ray<LAYOUT != LMGPU_LAYOUT_NAIVE>(r, in);   // a render ray (the naive scan keeps the exact setup)
     h.tri = -1;
     if (s.num_tris == 0) return -1;
     bool ok;
-    if (LAYOUT == LMGPU_LAYOUT_BVH2) ok = trace_bvh2<ANY>(s.bvh2, s.tris, s.root_ref, s.root_box, r, h, stack, s.stack_cap < STACK ? s.stack_cap : STACK, nullptr);
-    else if (LAYOUT == LMGPU_LAYOUT_BVH4) ok = trace_bvh4<ANY>(s.bvh4, s.tris, s.root_ref4, s.root_box, r, h, stack, s.stack_cap < STACK ? s.stack_cap : STACK, nullptr);
+    const int cap = s.stack_cap < STACK ? s.stack_cap : STACK;
+    // The renderers' walks and triangle test: the wavefront kernels' own.
+    if (LAYOUT == LMGPU_LAYOUT_BVH2 && ANY && LMGPU_TRACE_ANYHIT_WALK)   // visibility: the any-hit walk
+        ok = trace_bvh2_any<true>(s.bvh2, s.tris, s.root_ref, s.root_box, r, h, reinterpret_cast<int*>(stack), cap, nullptr);
+    else if (LAYOUT == LMGPU_LAYOUT_BVH2) ok = trace_bvh2<ANY, true>(s.bvh2, s.tris, s.root_ref, s.root_box, r, h, stack, cap, nullptr);
+    else if (LAYOUT == LMGPU_LAYOUT_BVH4) ok = trace_bvh4<ANY, true>(s.bvh4, s.tris, s.root_ref4, s.root_box, r, h, stack, cap, nullptr);
     else { trace_naive<ANY>(s.tris_by_id, s.num_tris, r, h, nullptr); ok = true; }
     if (!ok) { atomicOr(status, STATUS_STACK_OVERFLOW); h.tri = -1; }
     return h.tri;
@@ -91,10 +110,25 @@ __device__ __forceinline__ V3 light_Le(const DeviceScene& s, const DiffConsts& c
     return c.emission ? load3(c.emission + 3 * li) : load3(s.area_lights[li].Le);
 }
 
+// Per-path records of the adjoint. w[i] (i < RECORDED_VERTS): the weights
+// of the contributions whose prefix ends at vertex i; w[TAIL_SUM]: all
+// contributions deeper than RECORDED_VERTS; w[RUN_SUM]: in the tail replay,
+// the tail contributions met so far. (One array, indexed at run time, so
+// that the sums stay in local memory rather than in registers.)
+constexpr int TAIL_SUM = RECORDED_VERTS, RUN_SUM = RECORDED_VERTS + 1;
 struct Replay {
-    int32_t tri[MAX_REPLAY_VERTS];
-    V3 w[MAX_REPLAY_VERTS];   // adjoint: weights of the contributions whose prefix ends at this vertex
-    int n;
+    int32_t tri[RECORDED_VERTS];
+    V3 w[RECORDED_VERTS + 2];
+};
+
+// A path between two bounces: everything the bounce loop carries, so that
+// the loop can resume from it.
+struct PathPoint {
+    V3 ro, rd, thr, prev_p, prev_n;
+    float tmin, prev_pdf;
+    int k;                    // index of the next bounce
+    int nv;                   // surface vertices so far
+    bool prev_deg, prev_spec;
 };
 
 // Emission gradient of one light summed by a thread; flushed into the
@@ -117,9 +151,11 @@ __device__ __forceinline__ void flush_emission(EmissionSum& e, float* s_de, floa
 }
 
 // One contribution: forward splats it, the adjoint records dL/dI . c for the
-// albedos of its prefix (prefix length `depth`) and for its light.
+// albedos of its prefix (prefix length `depth`) and for its light. In the
+// tail replay (`tail`) only contributions deeper than RECORDED_VERTS count,
+// into the running sum; their light's gradient was added by the main replay.
 template <bool BACKWARD>
-__device__ __forceinline__ void contribute(const DiffConsts& c, const DeviceScene& s, Replay& rp, int depth,
+__device__ __forceinline__ void contribute(const DiffConsts& c, const DeviceScene& s, Replay& rp, bool tail, int depth,
                                            int light, int pixel, V3 contrib, float* image, const float* dL,
                                            EmissionSum& es, float* s_de, float* d_emission)
 {
@@ -132,7 +168,14 @@ __device__ __forceinline__ void contribute(const DiffConsts& c, const DeviceScen
     }
     const V3 w = v3(dL[3 * pixel] * contrib.x, dL[3 * pixel + 1] * contrib.y, dL[3 * pixel + 2] * contrib.z) * c.scale;
     if (is_zero(w)) return;
-    if (depth > 0) rp.w[depth - 1] = rp.w[depth - 1] + w;
+    if (tail) {
+        if (depth > RECORDED_VERTS) rp.w[RUN_SUM] = rp.w[RUN_SUM] + w;
+        return;
+    }
+    if (depth > 0) {
+        const int slot = depth > RECORDED_VERTS ? TAIL_SUM : depth - 1;
+        rp.w[slot] = rp.w[slot] + w;
+    }
     if (light >= 0 && light < s.num_area_lights) {
         const V3 Le = light_Le(s, c, light);
         const V3 g = v3(Le.x != 0.0f ? w.x / Le.x : 0.0f, Le.y != 0.0f ? w.y / Le.y : 0.0f,
@@ -143,20 +186,27 @@ __device__ __forceinline__ void contribute(const DiffConsts& c, const DeviceScen
     }
 }
 
-// End of a replayed path: vertex i's albedo gradient is the sum of the
-// weights of every contribution whose prefix contains it (suffix sums).
-__device__ __forceinline__ void flush_albedo(const DiffConsts& c, const DeviceScene& s, const Replay& rp, float* d_albedo)
+// Adds weight S / R to the albedo gradient of triangle t (diffuse only).
+__device__ __forceinline__ void add_albedo_grad(const DiffConsts& c, const DeviceScene& s, int t, V3 S, float* d_albedo)
 {
-    V3 S = v3(0, 0, 0);
-    for (int i = rp.n - 1; i >= 0; i--) {
+    if (is_zero(S)) return;
+    const Material m = diff_material(s, c, t);
+    if (m.type != LMGPU_BSDF_DIFFUSE) return;
+    if (m.R.x != 0.0f) atomicAdd(d_albedo + 3 * (int64_t)t, S.x / m.R.x);
+    if (m.R.y != 0.0f) atomicAdd(d_albedo + 3 * (int64_t)t + 1, S.y / m.R.y);
+    if (m.R.z != 0.0f) atomicAdd(d_albedo + 3 * (int64_t)t + 2, S.z / m.R.z);
+}
+
+// End of a replayed path: the albedo gradient weight of recorded vertex i is
+// the sum of the weights of every contribution whose prefix contains it: the
+// suffix sum of the recorded weights plus every deeper contribution.
+__device__ __forceinline__ void flush_albedo(const DiffConsts& c, const DeviceScene& s, const Replay& rp, int n,
+                                             float* d_albedo)
+{
+    V3 S = rp.w[TAIL_SUM];
+    for (int i = n - 1; i >= 0; i--) {
         S = S + rp.w[i];
-        if (is_zero(S)) continue;
-        const int t = rp.tri[i];
-        const Material m = diff_material(s, c, t);
-        if (m.type != LMGPU_BSDF_DIFFUSE) continue;
-        if (m.R.x != 0.0f) atomicAdd(d_albedo + 3 * (int64_t)t, S.x / m.R.x);
-        if (m.R.y != 0.0f) atomicAdd(d_albedo + 3 * (int64_t)t + 1, S.y / m.R.y);
-        if (m.R.z != 0.0f) atomicAdd(d_albedo + 3 * (int64_t)t + 2, S.z / m.R.z);
+        add_albedo_grad(c, s, rp.tri[i], S, d_albedo);
     }
 }
 
@@ -168,6 +218,122 @@ __device__ __forceinline__ int sample_light_diff(const DeviceScene& s, const Dif
     const int li = min(static_cast<int>(u0 * float(nl)), nl - 1);
     lp.Le = light_Le(s, c, li);
     return li;
+}
+
+// Saves the checkpoint. Kept out of line: the copy runs once per deep path,
+// and inlined it costs the bounce loop registers (backward 36.6 -> 34.5 ms
+// on the refined Cornell box out of line).
+__device__ __noinline__ void save_point(PathPoint* dst, const PathPoint& src) { *dst = src; }
+
+// The bounce loop from `pp` until the path ends. TAIL is the adjoint's
+// second replay of a deep path's tail; otherwise, in the adjoint, the state
+// on arrival at depth RECORDED_VERTS is saved in *ck and *deep set. Both
+// instantiations compute the same path from the same state.
+template <int TECH, int LAYOUT, int STACK, bool BACKWARD, bool TAIL>
+__device__ __forceinline__ void bounce_loop(const DeviceScene& s, const DiffConsts& c, uint64_t key, int path_pixel,
+                                            PathPoint& pp, PathPoint* ck, bool* deep, Replay& rp, int2* stack,
+                                            float* image, const float* dL, float* d_albedo, EmissionSum& es,
+                                            float* s_de, float* d_emission, int32_t* status)
+{
+    for (;;) {
+        if (c.max_pv != -1 && pp.k >= c.max_pv) break;
+        if (BACKWARD && !TAIL && pp.nv == RECORDED_VERTS) { save_point(ck, pp); *deep = true; }
+        Hit h;
+        const int tri = cast_ray<LAYOUT, false, STACK>(s, pp.ro, pp.rd, pp.tmin, FLT_MAX, h, stack, status);
+        Geom g;
+        const V3 wi = -pp.rd;
+        V3 Le = v3(0, 0, 0);
+        float lpdf = 0.0f;
+        int light = -1;
+        bool surface = false;
+        Material m;
+        m.type = LMGPU_BSDF_BLACK;
+        m.R = v3(0, 0, 0);
+        if (tri < 0) {
+            float t;
+            if (!(s.has_env && env_sphere_intersect(s, pp.ro, pp.rd, pp.tmin, FLT_MAX, t))) break;
+            env_surface(s, pp.ro, pp.rd, t, g);
+            Le = emitted(load3(s.env_Le), g.sn, wi);
+            lpdf = s.env_inv_area;
+            light = s.num_area_lights;
+        } else {
+            surface_from_hit(s, tri, h.u, h.v, pp.ro, pp.rd, h.t, g);
+            const int li = s.prim_light[s.tri_prim[tri]];
+            if (li >= 0) {
+                Le = emitted(light_Le(s, c, li), g.sn, wi);
+                lpdf = s.area_lights[li].inv_area;
+                light = li;
+            }
+            m = diff_material(s, c, tri);
+            surface = true;
+            if (pp.nv == MAX_PATH_VERTICES) {
+                atomicOr(status, STATUS_QUEUE_OVERFLOW);
+                break;
+            }
+            if (BACKWARD && !TAIL && pp.nv < RECORDED_VERTS) {
+                rp.tri[pp.nv] = tri;
+                rp.w[pp.nv] = v3(0, 0, 0);
+            }
+            pp.nv++;
+        }
+        const int depth_here = pp.nv - (surface ? 1 : 0);
+        if (!is_zero(Le)) {
+            const V3 contrib = pp.thr * Le;
+            if (TECH == LMGPU_RENDER_PT || pp.prev_spec) {
+                contribute<BACKWARD>(c, s, rp, TAIL, depth_here, light, path_pixel, contrib, image, dL, es, s_de,
+                                     d_emission);
+            } else if (TECH == LMGPU_RENDER_PT_MIS) {
+                const float G = geometry_term(pp.prev_p, pp.prev_n, pp.prev_deg, g.p, g.sn, false);
+                const float pdl = G == 0.0f ? 0.0f : lpdf / (float(s.num_lights) * G);
+                contribute<BACKWARD>(c, s, rp, TAIL, depth_here, light, path_pixel,
+                                     contrib * (pp.prev_pdf / (pp.prev_pdf + pdl)), image, dL, es, s_de, d_emission);
+            }
+        }
+        if (!surface) break;
+        // Tail replay: every tail contribution no deeper than this vertex
+        // has been met; the rest have it on their prefix.
+        if (BACKWARD && TAIL && pp.nv > RECORDED_VERTS) add_albedo_grad(c, s, tri, rp.w[TAIL_SUM] - rp.w[RUN_SUM], d_albedo);
+        const int v = pp.k + 1;
+        if (TECH != LMGPU_RENDER_PT && c.max_pv != -1 && v >= c.max_pv) break;
+        if (TECH != LMGPU_RENDER_PT && has_non_delta(m.type)) {
+            LightPoint lp;
+            const int li = sample_light_diff(s, c, rng_uniform(key, dim_vertex(v) + DIM_LIGHT),
+                                             rng_uniform(key, dim_vertex(v) + DIM_LIGHT + 1), lp);
+            if (li >= 0) {
+                const V3 ppL = normalize(lp.p - g.p);
+                float pb;
+                const V3 fs = eval_bsdf(m, g, wi, ppL, pb);
+                const float G = geometry_term(g.p, g.sn, false, lp.p, lp.n, false);
+                const V3 Lel = emitted(lp.Le, lp.n, -ppL);
+                if (G != 0.0f && !is_zero(fs) && !is_zero(Lel) && visible<LAYOUT, STACK>(s, g.p, lp.p, stack, status)) {
+                    float w = 1.0f;
+                    if (TECH == LMGPU_RENDER_PT_MIS) { const float pdl = lp.pdf_area / G; w = pdl / (pdl + pb); }
+                    contribute<BACKWARD>(c, s, rp, TAIL, pp.nv, li, path_pixel, pp.thr * fs * Lel * (w * G / lp.pdf_area),
+                                         image, dL, es, s_de, d_emission);
+                }
+            }
+        }
+        const int kv = TECH == LMGPU_RENDER_PT ? pp.k : v;
+        if (TECH != LMGPU_RENDER_PT && c.rr_depth != -1 && kv >= c.rr_depth) {
+            const float p = fminf(0.5f, luminance(pp.thr));
+            if (rng_uniform(key, dim_vertex(kv) + DIM_RR) > p) break;
+            pp.thr = pp.thr / p;
+        }
+        const BsdfSample bs = sample_bsdf(m, g, wi, rng_uniform(key, dim_vertex(kv) + DIM_BSDF),
+                                          rng_uniform(key, dim_vertex(kv) + DIM_BSDF + 1),
+                                          rng_uniform(key, dim_vertex(kv) + DIM_COMP));
+        if (is_zero(bs.weight)) break;
+        pp.thr = pp.thr * bs.weight;
+        if (TECH == LMGPU_RENDER_PT && c.rr_depth != -1 && pp.k >= c.rr_depth) {
+            const float p = fminf(0.5f, luminance(pp.thr));
+            if (rng_uniform(key, dim_vertex(pp.k) + DIM_RR) > p) break;
+            pp.thr = pp.thr / p;
+        }
+        if (TECH == LMGPU_RENDER_PT && c.max_pv != -1 && pp.k + 1 >= c.max_pv) break;
+        pp.prev_p = g.p; pp.prev_n = g.sn; pp.prev_deg = false; pp.prev_spec = bs.specular; pp.prev_pdf = bs.pdf;
+        pp.ro = g.p; pp.rd = bs.wo; pp.tmin = EPS_F;
+        pp.k++;
+    }
 }
 
 template <int TECH, int LAYOUT, int STACK, bool BACKWARD>
@@ -193,7 +359,10 @@ __global__ void __launch_bounds__(128, 8) k_diff(const DeviceScene s, const Diff
     for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < c.num_samples; j += stride) {
         const uint64_t sample = (uint64_t)(c.sample_offset + j);
         const uint64_t key = sample_key(c.seed, sample);
-        rp.n = 0;
+        if (BACKWARD) {
+            rp.w[TAIL_SUM] = v3(0, 0, 0);
+            rp.w[RUN_SUM] = v3(0, 0, 0);
+        }
         const float u0 = rng_uniform(key, DIM_RASTER), u1 = rng_uniform(key, DIM_RASTER + 1);
         float rx, ry;
         if (c.sampling == LMGPU_SAMPLING_STRATIFIED) {
@@ -207,12 +376,15 @@ __global__ void __launch_bounds__(128, 8) k_diff(const DeviceScene s, const Diff
         float pdf_cam;
         const V3 dir = camera_direction(s.cam, rx, ry, pdf_cam);
         const V3 cp = load3(s.cam.position);
-        V3 thr = v3(1, 1, 1);
         if (c.max_pv != -1 && c.max_pv <= 1) continue;
-        V3 prev_p = cp, prev_n = v3(0, 0, 1);
-        bool prev_deg = true, prev_spec = false;
-        float prev_pdf = pdf_cam;
-        float tmin = TECH == LMGPU_RENDER_PT ? 0.0f : EPS_F;
+        PathPoint pp;
+        pp.ro = cp; pp.rd = dir; pp.thr = v3(1, 1, 1);
+        pp.prev_p = cp; pp.prev_n = v3(0, 0, 1);
+        pp.prev_deg = true; pp.prev_spec = false;
+        pp.prev_pdf = pdf_cam;
+        pp.tmin = TECH == LMGPU_RENDER_PT ? 0.0f : EPS_F;
+        pp.k = 1;
+        pp.nv = 0;
         bool alive = true;
         if (TECH != LMGPU_RENDER_PT) {
             LightPoint lp;
@@ -227,111 +399,30 @@ __global__ void __launch_bounds__(128, 8) k_diff(const DeviceScene s, const Diff
                     if (G != 0.0f && !is_zero(Le) && visible<LAYOUT, STACK>(s, cp, lp.p, stack, status)) {
                         float w = 1.0f;
                         if (TECH == LMGPU_RENDER_PT_MIS) { const float pdl = lp.pdf_area / G; w = pdl / (pdl + We); }
-                        contribute<BACKWARD>(c, s, rp, 0, li, film_pixel(s.cam, lrx, lry), Le * (w * We * G / lp.pdf_area),
-                                             image, dL, es, s_de, d_emission);
+                        contribute<BACKWARD>(c, s, rp, false, 0, li, film_pixel(s.cam, lrx, lry),
+                                             Le * (w * We * G / lp.pdf_area), image, dL, es, s_de, d_emission);
                     }
                 }
             }
             if (c.rr_depth != -1 && 1 >= c.rr_depth) {
-                const float p = fminf(0.5f, luminance(thr));
+                const float p = fminf(0.5f, luminance(pp.thr));
                 if (rng_uniform(key, dim_vertex(1) + DIM_RR) > p) alive = false;
-                else thr = thr / p;
+                else pp.thr = pp.thr / p;
             }
         }
-        V3 ro = cp, rd = dir;
-        for (int k = 1; alive; k++) {
-            if (c.max_pv != -1 && k >= c.max_pv) break;
-            Hit h;
-            const int tri = cast_ray<LAYOUT, false, STACK>(s, ro, rd, tmin, FLT_MAX, h, stack, status);
-            Geom g;
-            const V3 wi = -rd;
-            V3 Le = v3(0, 0, 0);
-            float lpdf = 0.0f;
-            int light = -1;
-            bool surface = false;
-            Material m;
-            m.type = LMGPU_BSDF_BLACK;
-            m.R = v3(0, 0, 0);
-            if (tri < 0) {
-                float t;
-                if (!(s.has_env && env_sphere_intersect(s, ro, rd, tmin, FLT_MAX, t))) break;
-                env_surface(s, ro, rd, t, g);
-                Le = emitted(load3(s.env_Le), g.sn, wi);
-                lpdf = s.env_inv_area;
-                light = s.num_area_lights;
-            } else {
-                surface_from_hit(s, tri, h.u, h.v, ro, rd, h.t, g);
-                const int li = s.prim_light[s.tri_prim[tri]];
-                if (li >= 0) {
-                    Le = emitted(light_Le(s, c, li), g.sn, wi);
-                    lpdf = s.area_lights[li].inv_area;
-                    light = li;
-                }
-                m = diff_material(s, c, tri);
-                surface = true;
-                if (rp.n < MAX_REPLAY_VERTS) {
-                    rp.tri[rp.n] = tri;
-                    if (BACKWARD) rp.w[rp.n] = v3(0, 0, 0);
-                    rp.n++;
-                } else {
-                    atomicOr(status, STATUS_QUEUE_OVERFLOW);
-                    break;
-                }
-            }
-            const int depth_here = rp.n - (surface ? 1 : 0);
-            if (!is_zero(Le)) {
-                const V3 contrib = thr * Le;
-                if (TECH == LMGPU_RENDER_PT || prev_spec) {
-                    contribute<BACKWARD>(c, s, rp, depth_here, light, path_pixel, contrib, image, dL, es, s_de, d_emission);
-                } else if (TECH == LMGPU_RENDER_PT_MIS) {
-                    const float G = geometry_term(prev_p, prev_n, prev_deg, g.p, g.sn, false);
-                    const float pdl = G == 0.0f ? 0.0f : lpdf / (float(s.num_lights) * G);
-                    contribute<BACKWARD>(c, s, rp, depth_here, light, path_pixel, contrib * (prev_pdf / (prev_pdf + pdl)),
-                                         image, dL, es, s_de, d_emission);
-                }
-            }
-            if (!surface) break;
-            const int v = k + 1;
-            if (TECH != LMGPU_RENDER_PT && c.max_pv != -1 && v >= c.max_pv) break;
-            if (TECH != LMGPU_RENDER_PT && has_non_delta(m.type)) {
-                LightPoint lp;
-                const int li = sample_light_diff(s, c, rng_uniform(key, dim_vertex(v) + DIM_LIGHT),
-                                                 rng_uniform(key, dim_vertex(v) + DIM_LIGHT + 1), lp);
-                if (li >= 0) {
-                    const V3 ppL = normalize(lp.p - g.p);
-                    float pb;
-                    const V3 fs = eval_bsdf(m, g, wi, ppL, pb);
-                    const float G = geometry_term(g.p, g.sn, false, lp.p, lp.n, false);
-                    const V3 Lel = emitted(lp.Le, lp.n, -ppL);
-                    if (G != 0.0f && !is_zero(fs) && !is_zero(Lel) && visible<LAYOUT, STACK>(s, g.p, lp.p, stack, status)) {
-                        float w = 1.0f;
-                        if (TECH == LMGPU_RENDER_PT_MIS) { const float pdl = lp.pdf_area / G; w = pdl / (pdl + pb); }
-                        contribute<BACKWARD>(c, s, rp, rp.n, li, path_pixel, thr * fs * Lel * (w * G / lp.pdf_area),
-                                             image, dL, es, s_de, d_emission);
-                    }
-                }
-            }
-            const int kv = TECH == LMGPU_RENDER_PT ? k : v;
-            if (TECH != LMGPU_RENDER_PT && c.rr_depth != -1 && kv >= c.rr_depth) {
-                const float p = fminf(0.5f, luminance(thr));
-                if (rng_uniform(key, dim_vertex(kv) + DIM_RR) > p) break;
-                thr = thr / p;
-            }
-            const BsdfSample bs = sample_bsdf(m, g, wi, rng_uniform(key, dim_vertex(kv) + DIM_BSDF),
-                                              rng_uniform(key, dim_vertex(kv) + DIM_BSDF + 1),
-                                              rng_uniform(key, dim_vertex(kv) + DIM_COMP));
-            if (is_zero(bs.weight)) break;
-            thr = thr * bs.weight;
-            if (TECH == LMGPU_RENDER_PT && c.rr_depth != -1 && k >= c.rr_depth) {
-                const float p = fminf(0.5f, luminance(thr));
-                if (rng_uniform(key, dim_vertex(k) + DIM_RR) > p) break;
-                thr = thr / p;
-            }
-            if (TECH == LMGPU_RENDER_PT && c.max_pv != -1 && k + 1 >= c.max_pv) break;
-            prev_p = g.p; prev_n = g.sn; prev_deg = false; prev_spec = bs.specular; prev_pdf = bs.pdf;
-            ro = g.p; rd = bs.wo; tmin = EPS_F;
+        PathPoint ck;
+        bool deep = false;
+        if (alive)
+            bounce_loop<TECH, LAYOUT, STACK, BACKWARD, false>(s, c, key, path_pixel, pp, &ck, &deep, rp, stack, image, dL,
+                                                              d_albedo, es, s_de, d_emission, status);
+        if (BACKWARD) {
+            flush_albedo(c, s, rp, min(pp.nv, RECORDED_VERTS), d_albedo);
+            // The tail of a path deeper than RECORDED_VERTS: replayed from the
+            // checkpoint taken on arrival at that depth.
+            if (deep)
+                bounce_loop<TECH, LAYOUT, STACK, BACKWARD, true>(s, c, key, path_pixel, ck, nullptr, nullptr, rp, stack,
+                                                                 image, dL, d_albedo, es, s_de, d_emission, status);
         }
-        if (BACKWARD) flush_albedo(c, s, rp, d_albedo);
     }
     if (BACKWARD) {
         flush_emission(es, s_de, d_emission);
@@ -347,8 +438,8 @@ int launch_diff_l(LmgpuScene* sc, const DiffConsts& c, bool backward, float* ima
                   float* de, cudaStream_t st)
 {
     const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((c.num_samples + 127) / 128, 148 * 16));
-    if (backward) k_diff<TECH, LAYOUT, STACK, true><<<blocks, 128, 0, st>>>(sc->dev, c, image, dL, da, de, sc->d_status);
-    else k_diff<TECH, LAYOUT, STACK, false><<<blocks, 128, 0, st>>>(sc->dev, c, image, dL, da, de, sc->d_status);
+    if (backward) k_diff<TECH, LAYOUT, STACK, true><<<blocks, 128, 0, st>>>(sc->rdev, c, image, dL, da, de, sc->d_status);
+    else k_diff<TECH, LAYOUT, STACK, false><<<blocks, 128, 0, st>>>(sc->rdev, c, image, dL, da, de, sc->d_status);
     LMGPU_CUDA_TRY(cudaGetLastError());
     return LMGPU_OK;
 }
@@ -368,7 +459,7 @@ template <int TECH>
 int launch_diff_t(LmgpuScene* sc, const DiffConsts& c, bool backward, float* image, const float* dL, float* da,
                   float* de, cudaStream_t st)
 {
-    const int cap = sc->dev.stack_cap;
+    const int cap = sc->rdev.stack_cap;
     if (cap <= 32) return launch_diff_s<TECH, 32>(sc, c, backward, image, dL, da, de, st);
     if (cap <= 64) return launch_diff_s<TECH, 64>(sc, c, backward, image, dL, da, de, st);
     if (cap <= 128) return launch_diff_s<TECH, 128>(sc, c, backward, image, dL, da, de, st);

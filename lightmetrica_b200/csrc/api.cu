@@ -170,6 +170,8 @@ int create_impl(const LmgpuSceneDesc* desc, LmgpuScene** out)
     if (desc->num_primitives < 0 || (desc->num_primitives > 0 && !desc->primitives))
         return fail(LMGPU_ERR_INVALID, "bad primitive list");
     if (desc->max_stack_entries < 0) return fail(LMGPU_ERR_INVALID, "negative traversal stack bound");
+    if (desc->render_tree != LMGPU_RENDER_TREE_SAH && desc->render_tree != LMGPU_RENDER_TREE_REFERENCE)
+        return fail(LMGPU_ERR_INVALID, "unknown render tree");
     if (desc->layout < LMGPU_LAYOUT_BVH2 || desc->layout > LMGPU_LAYOUT_NAIVE)
         return fail(LMGPU_ERR_INVALID, "unknown layout");
     for (int i = 0; i < desc->num_primitives; i++) {
@@ -197,6 +199,15 @@ int create_impl(const LmgpuSceneDesc* desc, LmgpuScene** out)
         return fail(LMGPU_ERR_OOM, "host allocation failed during the BVH build");
     }
     if (!err.empty()) return fail(LMGPU_ERR_INVALID, err);
+    const bool render_tree = desc->layout != LMGPU_LAYOUT_NAIVE && desc->render_tree == LMGPU_RENDER_TREE_SAH &&
+                             b.num_tris > 0;
+    if (render_tree) {
+        try {
+            build_render_tree(b, desc->build_threads);
+        } catch (const std::bad_alloc&) {
+            return fail(LMGPU_ERR_OOM, "host allocation failed during the render tree build");
+        }
+    }
 
     CameraGpu cam;
     if (!setup_camera(*desc, cam)) return fail(LMGPU_ERR_INVALID, "invalid camera");
@@ -300,6 +311,19 @@ int create_impl(const LmgpuSceneDesc* desc, LmgpuScene** out)
         d.env_radius = float(std::sqrt(r2));
         d.env_inv_area = float(1.0 / (4.0 * 3.14159265358979323846 * r2));
     }
+    // Render view: the same scene with the render tree's accelerator.
+    s->rdev = d;
+    if (render_tree) {
+        DeviceScene& r = s->rdev;
+        up(b.rtris, &r.tris);
+        up(b.rbvh2, &r.bvh2);
+        up(b.rbvh4, &r.bvh4);
+        r.root_ref = b.rbvh2_root;
+        r.root_ref4 = b.rbvh4_root;
+        std::memcpy(r.root_box, b.rroot_box, sizeof(r.root_box));
+        r.stack_cap = 2 * b.rmax_depth + 4;
+        if (desc->max_stack_entries > 0 && desc->max_stack_entries < r.stack_cap) r.stack_cap = desc->max_stack_entries;
+    }
     if (rc != LMGPU_OK) { lmgpu_scene_destroy(s); return rc; }
 
     // Scratch: status word and the persistent kernels' work counter.
@@ -322,8 +346,17 @@ int create_impl(const LmgpuSceneDesc* desc, LmgpuScene** out)
     int64_t bytes = 0;
     bytes += (int64_t)b.tris.size() * sizeof(TriRecord);
     bytes += (desc->layout == LMGPU_LAYOUT_BVH4 ? (int64_t)b.bvh4.size() * sizeof(Bvh4Node) : (int64_t)b.bvh2.size() * sizeof(Bvh2Node));
+    if (render_tree) {
+        bytes += (int64_t)b.rtris.size() * sizeof(TriRecord);
+        bytes += (desc->layout == LMGPU_LAYOUT_BVH4 ? (int64_t)b.rbvh4.size() * sizeof(Bvh4Node) : (int64_t)b.rbvh2.size() * sizeof(Bvh2Node));
+    }
     info.device_bytes = bytes;
     for (int c = 0; c < 3; c++) { info.bounds_min[c] = b.bounds.mn[c]; info.bounds_max[c] = b.bounds.mx[c]; }
+    info.render_tree = render_tree ? LMGPU_RENDER_TREE_SAH : LMGPU_RENDER_TREE_REFERENCE;
+    info.render_max_depth = render_tree ? b.rmax_depth : b.max_depth;
+    info.render_num_nodes = render_tree ? b.rnum_nodes : static_cast<int64_t>(b.nodes.size());
+    info.render_num_leaves = render_tree ? b.rnum_leaves : b.num_leaves;
+    info.render_build_seconds = render_tree ? b.rbuild_seconds : 0.0;
     *out = s;
     return LMGPU_OK;
 }
@@ -747,6 +780,24 @@ int lmgpu_scene_build_host(const LmgpuSceneDesc* desc, LmgpuSceneInfo* info, int
                          (desc->layout == LMGPU_LAYOUT_BVH4 ? (int64_t)b.bvh4.size() * sizeof(Bvh4Node)
                                                             : (int64_t)b.bvh2.size() * sizeof(Bvh2Node));
     for (int c = 0; c < 3; c++) { info->bounds_min[c] = b.bounds.mn[c]; info->bounds_max[c] = b.bounds.mx[c]; }
+    // The render tree, as lmgpu_scene_create builds it.
+    if (desc->layout != LMGPU_LAYOUT_NAIVE && desc->render_tree == LMGPU_RENDER_TREE_SAH && b.num_tris > 0) {
+        try {
+            build_render_tree(b, desc->build_threads);
+        } catch (const std::bad_alloc&) {
+            return fail(LMGPU_ERR_OOM, "host allocation failed during the render tree build");
+        }
+        info->render_tree = LMGPU_RENDER_TREE_SAH;
+        info->render_max_depth = b.rmax_depth;
+        info->render_num_nodes = b.rnum_nodes;
+        info->render_num_leaves = b.rnum_leaves;
+        info->render_build_seconds = b.rbuild_seconds;
+    } else {
+        info->render_tree = LMGPU_RENDER_TREE_REFERENCE;
+        info->render_max_depth = b.max_depth;
+        info->render_num_nodes = info->num_nodes;
+        info->render_num_leaves = b.num_leaves;
+    }
     if (tri_order) {
         if (capacity < b.num_tris) return fail(LMGPU_ERR_INVALID, "tri_order capacity too small");
         std::memcpy(tri_order, b.tri_order.data(), (size_t)b.num_tris * sizeof(int32_t));

@@ -492,7 +492,7 @@ int make_plan(LmgpuBatch* b, const LmgpuRenderParams* params, void* const* films
         pl.total += p.num_samples;
         if (p.max_path_vertices == -1) pl.bounded = false;
         else max_pv = std::max(max_pv, p.max_path_vertices);
-        cap = std::max(cap, sc->dev.stack_cap);
+        cap = std::max(cap, sc->rdev.stack_cap);
     }
     if (pl.total >= (int64_t(1) << 62)) return fail(LMGPU_ERR_INVALID, "sample count too large");
     pl.bounces = pl.bounded ? max_pv - 1 : GRAPH_BOUNCES_UNBOUNDED;
@@ -516,7 +516,7 @@ int upload_table(LmgpuBatch* b, const LmgpuRenderParams* params, void* const* fi
     for (int i = 0; i < n; i++) {
         const LmgpuRenderParams& p = params[i];
         BatchEntry& e = b->h_table[i];
-        e.s = b->scenes[i]->dev;
+        e.s = b->scenes[i]->rdev;
         e.s.layout = b->cfg.layout;
         e.rc.technique = p.technique;
         e.rc.rr_depth = p.rr_depth;
@@ -546,7 +546,7 @@ int run_stream(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_t
     Launch L;
     L.paths = P;
     L.shade_blocks = std::max(1, b->cfg.shade_blocks_per_sm) * b->sms;
-    L.proto = b->scenes[0]->dev;
+    L.proto = b->scenes[0]->rdev;
     L.proto.layout = LAYOUT;
     L.proto.stack_cap = STACK;        // every scene of the batch: the largest bound
     S::warm(L);
@@ -607,7 +607,7 @@ int run_overlap(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_
     Launch L;
     L.paths = P;
     L.shade_blocks = std::max(1, b->cfg.shade_blocks_per_sm) * b->sms;
-    L.proto = b->scenes[0]->dev;
+    L.proto = b->scenes[0]->rdev;
     L.proto.layout = LAYOUT;
     L.proto.stack_cap = STACK;        // every scene of the batch: the largest bound
     W::warm(L);
@@ -690,7 +690,7 @@ int run_waves(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_t&
     Launch L;
     L.paths = P;
     L.shade_blocks = std::max(1, b->cfg.shade_blocks_per_sm) * b->sms;
-    L.proto = b->scenes[0]->dev;
+    L.proto = b->scenes[0]->rdev;
     L.proto.layout = LAYOUT;
     L.proto.stack_cap = STACK;        // every scene of the batch: the largest bound
     W::warm(L);

@@ -215,14 +215,14 @@ struct Builder {
 };
 
 // DFS pre-order flatten into Bvh2Node (internal nodes only).
-int32_t flatten_bvh2(const BuiltScene& s, int32_t ni, std::vector<Bvh2Node>& out)
+int32_t flatten_bvh2(const std::vector<BuildNode>& nodes, int32_t ni, std::vector<Bvh2Node>& out)
 {
-    const BuildNode& n = s.nodes[ni];
+    const BuildNode& n = nodes[ni];
     if (n.leaf) return ~n.begin;
     const int32_t id = static_cast<int32_t>(out.size());
     out.emplace_back();
-    const BuildNode& L = s.nodes[n.left];
-    const BuildNode& R = s.nodes[n.right];
+    const BuildNode& L = nodes[n.left];
+    const BuildNode& R = nodes[n.right];
     {
         Bvh2Node& o = out[id];
         o.bx[0] = L.bound.mn[0]; o.bx[1] = L.bound.mx[0]; o.bx[2] = R.bound.mn[0]; o.bx[3] = R.bound.mx[0];
@@ -231,8 +231,8 @@ int32_t flatten_bvh2(const BuiltScene& s, int32_t ni, std::vector<Bvh2Node>& out
         o.axis = n.axis;
         o.pad = 0;
     }
-    const int32_t l = flatten_bvh2(s, n.left, out);
-    const int32_t r = flatten_bvh2(s, n.right, out);
+    const int32_t l = flatten_bvh2(nodes, n.left, out);
+    const int32_t r = flatten_bvh2(nodes, n.right, out);
     out[id].left = l;
     out[id].right = r;
     return id;
@@ -241,9 +241,9 @@ int32_t flatten_bvh2(const BuiltScene& s, int32_t ni, std::vector<Bvh2Node>& out
 // 4-wide collapse: each 4-node holds the (up to) four grandchildren of a
 // binary internal node; a binary child that is a leaf occupies its slot pair
 // alone.
-int32_t flatten_bvh4(const BuiltScene& s, int32_t ni, std::vector<Bvh4Node>& out)
+int32_t flatten_bvh4(const std::vector<BuildNode>& nodes, int32_t ni, std::vector<Bvh4Node>& out)
 {
-    const BuildNode& n = s.nodes[ni];
+    const BuildNode& n = nodes[ni];
     if (n.leaf) return ~n.begin;
     const int32_t id = static_cast<int32_t>(out.size());
     out.emplace_back();
@@ -251,7 +251,7 @@ int32_t flatten_bvh4(const BuiltScene& s, int32_t ni, std::vector<Bvh4Node>& out
     int32_t axis_pair[2] = { -1, -1 };
     const int32_t kids[2] = { n.left, n.right };
     for (int p = 0; p < 2; p++) {
-        const BuildNode& c = s.nodes[kids[p]];
+        const BuildNode& c = nodes[kids[p]];
         if (c.leaf) { slot_node[2 * p] = kids[p]; }
         else { slot_node[2 * p] = c.left; slot_node[2 * p + 1] = c.right; axis_pair[p] = c.axis; }
     }
@@ -265,7 +265,7 @@ int32_t flatten_bvh4(const BuiltScene& s, int32_t ni, std::vector<Bvh4Node>& out
                 o.child[k] = BVH4_EMPTY;
                 continue;
             }
-            const HostAabb& b = s.nodes[slot_node[k]].bound;
+            const HostAabb& b = nodes[slot_node[k]].bound;
             o.lox[k] = b.mn[0]; o.hix[k] = b.mx[0];
             o.loy[k] = b.mn[1]; o.hiy[k] = b.mx[1];
             o.loz[k] = b.mn[2]; o.hiz[k] = b.mx[2];
@@ -276,11 +276,183 @@ int32_t flatten_bvh4(const BuiltScene& s, int32_t ni, std::vector<Bvh4Node>& out
         o.pad = 0;
     }
     for (int k = 0; k < 4; k++)
-        if (slot_node[k] >= 0) out[id].child[k] = flatten_bvh4(s, slot_node[k], out);
+        if (slot_node[k] >= 0) out[id].child[k] = flatten_bvh4(nodes, slot_node[k], out);
     return id;
 }
 
+// ------------------------------------------------------------ render tree
+
+// Render tree: binned SAH over all three axes (the reference bins only the
+// longest axis of the centroid bounds, into 12 buckets), cost
+// RTREE_NODE_COST + (nL AL + nR AR) / A in units of one triangle test
+// against a leaf's n, leaves of at most RTREE_MAX_LEAF triangles (unless
+// their centroids coincide).
+#ifndef LMGPU_RTREE_BINS
+#define LMGPU_RTREE_BINS 32
+#endif
+#ifndef LMGPU_RTREE_NODE_COST
+#define LMGPU_RTREE_NODE_COST 0.5f    // a node visit costs about half a triangle test (measured)
+#endif
+#ifndef LMGPU_RTREE_MAX_LEAF
+#define LMGPU_RTREE_MAX_LEAF 8
+#endif
+
+struct RenderBuilder {
+    static constexpr int NB = LMGPU_RTREE_BINS;
+    const std::vector<HostAabb>& tri_bounds;
+    const std::vector<float>& centroids;
+    std::vector<int32_t> order;
+    std::vector<BuildNode> pool;
+    std::atomic<int32_t> pool_next{0};
+    std::atomic<int64_t> leaves{0};
+    std::atomic<int32_t> depth{0};
+    int spawn_depth = 0;
+
+    RenderBuilder(const std::vector<HostAabb>& tb, const std::vector<float>& c) : tri_bounds(tb), centroids(c) {}
+
+    int32_t alloc_node() { return pool_next.fetch_add(1); }
+
+    int32_t make_leaf(int begin, int end, const HostAabb& bound)
+    {
+        int32_t id = alloc_node();
+        BuildNode& n = pool[id];
+        n.leaf = true; n.begin = begin; n.end = end; n.bound = bound;
+        leaves.fetch_add(1);
+        return id;
+    }
+
+    static int bin_of(float c, float lo, float scale)
+    {
+        const int b = static_cast<int>((c - lo) * scale);
+        return b < 0 ? 0 : (b >= NB ? NB - 1 : b);
+    }
+
+    int32_t build(int begin, int end, int d)
+    {
+        int32_t cur = depth.load();
+        while (d > cur && !depth.compare_exchange_weak(cur, d)) {}
+        HostAabb bound = aabb_empty(), cb = aabb_empty();
+        for (int i = begin; i < end; i++) {
+            aabb_grow(bound, tri_bounds[order[i]]);
+            aabb_grow_p(cb, &centroids[3 * (size_t)order[i]]);
+        }
+        const int n = end - begin;
+        if (n == 1) return make_leaf(begin, end, bound);
+        const float area = aabb_area(bound);
+        float best = FLT_MAX;
+        int best_axis = -1, best_bin = 0;
+        for (int axis = 0; axis < 3; axis++) {
+            const float lo = cb.mn[axis], ext = cb.mx[axis] - cb.mn[axis];
+            if (!(ext > 0.0f)) continue;
+            const float scale = float(NB) / ext;
+            HostAabb bb[NB];
+            int bc[NB];
+            for (int i = 0; i < NB; i++) { bb[i] = aabb_empty(); bc[i] = 0; }
+            for (int i = begin; i < end; i++) {
+                const int32_t t = order[i];
+                const int b = bin_of(centroids[3 * (size_t)t + axis], lo, scale);
+                bc[b]++;
+                aabb_grow(bb[b], tri_bounds[t]);
+            }
+            float right_area[NB];
+            int right_count[NB];
+            HostAabb acc = aabb_empty();
+            int c = 0;
+            for (int i = NB - 1; i >= 1; i--) {
+                aabb_grow(acc, bb[i]);
+                c += bc[i];
+                right_area[i] = aabb_area(acc);
+                right_count[i] = c;
+            }
+            acc = aabb_empty();
+            c = 0;
+            for (int i = 0; i < NB - 1; i++) {         // split after bin i
+                aabb_grow(acc, bb[i]);
+                c += bc[i];
+                if (c == 0 || right_count[i + 1] == 0) continue;
+                const float cost = LMGPU_RTREE_NODE_COST +
+                                   (float(c) * aabb_area(acc) + float(right_count[i + 1]) * right_area[i + 1]) / area;
+                if (cost < best) { best = cost; best_axis = axis; best_bin = i; }
+            }
+        }
+        if (best_axis < 0 || (n <= LMGPU_RTREE_MAX_LEAF && float(n) <= best)) return make_leaf(begin, end, bound);
+        const float lo = cb.mn[best_axis], scale = float(NB) / (cb.mx[best_axis] - cb.mn[best_axis]);
+        int32_t* o = order.data();
+        const int32_t* mid_ptr = std::partition(o + begin, o + end, [&](int32_t t) {
+            return bin_of(centroids[3 * (size_t)t + best_axis], lo, scale) <= best_bin;
+        });
+        const int mid = static_cast<int>(mid_ptr - o);
+        int32_t l, r;
+        if (d < spawn_depth && n > 4096) {
+            int32_t lres = -1;
+            std::thread th([&] { lres = build(begin, mid, d + 1); });
+            r = build(mid, end, d + 1);
+            th.join();
+            l = lres;
+        } else {
+            l = build(begin, mid, d + 1);
+            r = build(mid, end, d + 1);
+        }
+        int32_t id = alloc_node();
+        BuildNode& nd = pool[id];
+        nd.leaf = false; nd.axis = best_axis; nd.left = l; nd.right = r;
+        nd.bound = pool[l].bound;
+        aabb_grow(nd.bound, pool[r].bound);
+        return id;
+    }
+};
+
 }  // namespace
+
+void build_render_tree(BuiltScene& s, int threads)
+{
+    auto t0 = std::chrono::steady_clock::now();
+    const int64_t ntris = s.num_tris;
+    if (ntris <= 0) return;
+    std::vector<HostAabb> tb((size_t)ntris);
+    std::vector<float> cen(3 * (size_t)ntris);
+    for (int64_t t = 0; t < ntris; t++) {
+        const float* p1 = &s.positions[3 * (size_t)s.tri_vidx[3 * t]];
+        const float* p2 = &s.positions[3 * (size_t)s.tri_vidx[3 * t + 1]];
+        const float* p3 = &s.positions[3 * (size_t)s.tri_vidx[3 * t + 2]];
+        HostAabb b;
+        for (int c = 0; c < 3; c++) { b.mn[c] = min_sse(p1[c], p2[c]); b.mx[c] = max_sse(p1[c], p2[c]); }
+        aabb_grow_p(b, p3);
+        tb[(size_t)t] = b;
+        for (int c = 0; c < 3; c++) cen[3 * (size_t)t + c] = (b.mn[c] + b.mx[c]) * 0.5f;
+    }
+    RenderBuilder B(tb, cen);
+    B.order.resize((size_t)ntris);
+    for (int64_t t = 0; t < ntris; t++) B.order[(size_t)t] = static_cast<int32_t>(t);
+    if (threads <= 0) threads = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+    while ((1 << B.spawn_depth) < threads) B.spawn_depth++;
+    B.spawn_depth += 1;
+    B.pool.resize(2 * (size_t)ntris);
+    const int32_t root = B.build(0, static_cast<int32_t>(ntris), 0);
+    B.pool.resize((size_t)B.pool_next.load());
+    // Records in the render tree's leaf order: the same TriAccel constants.
+    std::vector<TriRecord> by_id((size_t)ntris);
+    for (int64_t i = 0; i < ntris; i++) by_id[s.tris[(size_t)i].tri_id] = s.tris[(size_t)i];
+    s.rtris.resize((size_t)ntris);
+    for (int64_t i = 0; i < ntris; i++) {
+        s.rtris[(size_t)i] = by_id[(size_t)B.order[(size_t)i]];
+        s.rtris[(size_t)i].k_flags &= ~TRI_LAST_IN_LEAF;
+    }
+    for (auto& n : B.pool)
+        if (n.leaf) s.rtris[(size_t)(n.end - 1)].k_flags |= TRI_LAST_IN_LEAF;
+    s.rbvh2.clear();
+    s.rbvh2.reserve((size_t)std::max<int64_t>(1, ntris));
+    s.rbvh2_root = flatten_bvh2(B.pool, root, s.rbvh2);
+    s.rbvh4.clear();
+    s.rbvh4_root = flatten_bvh4(B.pool, root, s.rbvh4);
+    const HostAabb& rb = B.pool[root].bound;
+    for (int c = 0; c < 3; c++) { s.rroot_box[c] = rb.mn[c]; s.rroot_box[3 + c] = rb.mx[c]; }
+    s.rnum_nodes = (int64_t)B.pool.size();
+    s.rnum_leaves = B.leaves.load();
+    s.rmax_depth = B.depth.load();
+    s.has_render_tree = true;
+    s.rbuild_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
 
 std::string build_scene(const std::vector<PrimitiveInput>& prims, int threads, bool want_bvh, BuiltScene& s)
 {
@@ -410,9 +582,9 @@ std::string build_scene(const std::vector<PrimitiveInput>& prims, int threads, b
         for (auto& n : s.nodes)
             if (n.leaf) s.tris[(size_t)(n.end - 1)].k_flags |= TRI_LAST_IN_LEAF;
         s.bvh2.reserve((size_t)std::max<int64_t>(1, ntris));
-        s.bvh2_root = flatten_bvh2(s, s.root, s.bvh2);
+        s.bvh2_root = flatten_bvh2(s.nodes, s.root, s.bvh2);
         s.bvh4.reserve((size_t)std::max<int64_t>(1, ntris / 2));
-        s.bvh4_root = flatten_bvh4(s, s.root, s.bvh4);
+        s.bvh4_root = flatten_bvh4(s.nodes, s.root, s.bvh4);
         const HostAabb& rb = s.nodes[s.root].bound;
         for (int c = 0; c < 3; c++) { s.root_box[c] = rb.mn[c]; s.root_box[3 + c] = rb.mx[c]; }
         s.max_stack = s.max_depth + 2;

@@ -49,6 +49,20 @@ struct BuiltScene {
     int32_t bvh4_root = 0;
     int32_t max_stack = 0;            // traversal stack bound for this tree
     double build_seconds = 0.0;
+
+    // Render tree (build_render_tree): a second tree over the same TriAccel
+    // records, for the path tracer only.
+    bool has_render_tree = false;
+    std::vector<TriRecord> rtris;     // its leaf order
+    std::vector<Bvh2Node> rbvh2;
+    int32_t rbvh2_root = 0;
+    float rroot_box[6] = {0, 0, 0, 0, 0, 0};
+    std::vector<Bvh4Node> rbvh4;
+    int32_t rbvh4_root = 0;
+    int64_t rnum_nodes = 0;
+    int64_t rnum_leaves = 0;
+    int32_t rmax_depth = 0;
+    double rbuild_seconds = 0.0;
 };
 
 struct PrimitiveInput {
@@ -64,5 +78,10 @@ struct PrimitiveInput {
 // Builds everything; returns an empty string on success, else an error.
 std::string build_scene(const std::vector<PrimitiveInput>& prims, int threads, bool want_bvh,
                         BuiltScene& out);
+
+// Builds the render tree of a scene that build_scene built: a binned SAH
+// tree over all three axes, for rendering only (closest hits may differ
+// from the reference tree's at exact ties, never in expectation).
+void build_render_tree(BuiltScene& s, int threads);
 
 }  // namespace lmgpu

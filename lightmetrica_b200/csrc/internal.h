@@ -27,7 +27,8 @@ struct HostPipeline {
 };
 
 struct LmgpuScene {
-    lmgpu::DeviceScene dev{};
+    lmgpu::DeviceScene dev{};         // the reference's tree (intersection entry points)
+    lmgpu::DeviceScene rdev{};        // what renders traverse: `dev` with the render tree's accelerator
     LmgpuSceneInfo info{};
     std::vector<void*> allocations;   // device buffers owned by the scene
     int device = 0;

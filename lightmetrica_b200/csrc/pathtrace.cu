@@ -157,7 +157,7 @@ template <class F>
 int shadow_pass(LmgpuScene* sc, const PathState& st, const OneScene<F>& ctx, int64_t max_rays, cudaStream_t stream)
 {
     ShadowIO<OneScene<F>> io{ st.counters + 2, st.sh_o, st.sh_d, st.sh_c, st.L, ctx };
-    return launch_trace<true>(sc, io, max_rays, stream);
+    return launch_trace<true, ShadowIO<OneScene<F>>>(sc, io, max_rays, stream, nullptr, true);
 }
 
 int read_counts(Workspace& ws, cudaStream_t stream)
@@ -171,7 +171,7 @@ template <int TECH, class F>
 int render_waves(LmgpuScene* sc, const LmgpuRenderParams& p, F* film, cudaStream_t stream, LmgpuRenderStats& stats,
                  Workspace& ws)
 {
-    const DeviceScene& s = sc->dev;
+    const DeviceScene& s = sc->rdev;
     const int64_t pixels = (int64_t)s.cam.width * s.cam.height;
     int64_t P = p.wave_paths > 0 ? p.wave_paths : DEFAULT_WAVE_PATHS;
     P = std::min<int64_t>(P, p.num_samples);
@@ -215,7 +215,7 @@ int render_waves(LmgpuScene* sc, const LmgpuRenderParams& p, F* film, cudaStream
             stats.rays_traced += n;
             stats.max_bounces_run = std::max(stats.max_bounces_run, k);
             PathRayIO<false> io{ st.counters + qin, st.qo[qin], st.qd[qin], st.hit, nullptr };
-            rc = launch_trace<false>(sc, io, n, stream);
+            rc = launch_trace<false, PathRayIO<false>>(sc, io, n, stream, nullptr, true);
             if (rc != LMGPU_OK) break;
             LMGPU_CUDA_TRY(cudaMemsetAsync(st.counters + (1 - qin), 0, 4, stream));
             LMGPU_CUDA_TRY(cudaMemsetAsync(st.counters + 2, 0, 4, stream));

@@ -370,6 +370,7 @@ constexpr int PATH_QUEUE_EXIT_BELOW = LMGPU_PT_EXIT_BELOW;
 template <bool TABLE>
 struct PathRayIO {
     static constexpr bool PER_RAY_SCENE = TABLE;
+    static constexpr bool RENDER = true;
     static constexpr int REFILL_MIN = PATH_QUEUE_REFILL_MIN;
     static constexpr int EXIT_BELOW = PATH_QUEUE_EXIT_BELOW;
     const uint32_t* count_ptr;
@@ -400,6 +401,7 @@ struct PathRayIO {
 template <class Ctx>
 struct ShadowIO {
     static constexpr bool PER_RAY_SCENE = Ctx::TABLE;
+    static constexpr bool RENDER = true;
     static constexpr int REFILL_MIN = PATH_QUEUE_REFILL_MIN;
     static constexpr int EXIT_BELOW = PATH_QUEUE_EXIT_BELOW;
     const uint32_t* count_ptr;

@@ -37,8 +37,32 @@ struct TraversalRay {
 
 constexpr uint32_t RAY_FINITE_INV = 8u;
 
+// Render rays (RENDER_SLAB) keep inv_min = 1/d, clamped to +-1e18 so that it
+// stays finite, and inv_max = -o/d: a plane distance is then one
+// multiply-add, (lo - o)/d = fma(lo, 1/d, -o/d) (slab_render).
+#ifndef LMGPU_RENDER_FMA_SLAB
+#define LMGPU_RENDER_FMA_SLAB 1
+#endif
+
+template <bool RENDER = false>
 __device__ __forceinline__ void setup_ray(TraversalRay& r, const RayIn& in)
 {
+    if (RENDER && LMGPU_RENDER_FMA_SLAB) {
+        r.neg = RAY_FINITE_INV;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            r.o[c] = in.o[c];
+            r.d[c] = in.d[c];
+            float inv = __frcp_rn(in.d[c]);
+            if (!(fabsf(inv) <= 1e18f)) inv = copysignf(1e18f, in.d[c]);
+            r.inv_min[c] = inv;
+            r.inv_max[c] = -(in.o[c] * inv);
+            r.neg |= (in.d[c] < 0.0f ? 1u : 0u) << c;
+        }
+        r.tmin = in.tmin;
+        r.tmax = in.tmax;
+        return;
+    }
     r.neg = RAY_FINITE_INV;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
@@ -130,6 +154,61 @@ __device__ __forceinline__ bool slab_finite(const TraversalRay& r,
     return tn <= tf && tf > r.tmin;
 }
 
+// The slab test of render rays (setup_ray<true>): plane distances by packed
+// multiply-adds fma.rn.f32x2 (sm_100), near/far by min/max as slab_finite.
+// It rounds differently from the reference's test near box faces, which
+// renders (same expected image, not bit-exact hits) tolerate.
+__device__ __forceinline__ void plane_pair_fma(float lo, float hi, float inv, float noinv, float& a, float& b)
+{
+    asm("{\n\t.reg .b64 p, q, r;\n\t"
+        "mov.b64 p, {%2, %3};\n\t"
+        "mov.b64 q, {%4, %4};\n\t"
+        "mov.b64 r, {%5, %5};\n\t"
+        "fma.rn.f32x2 p, p, q, r;\n\t"
+        "mov.b64 {%0, %1}, p;\n\t}"
+        : "=f"(a), "=f"(b) : "f"(lo), "f"(hi), "f"(inv), "f"(noinv));
+}
+
+__device__ __forceinline__ bool slab_render(const TraversalRay& r,
+                                            float lox, float hix, float loy, float hiy,
+                                            float loz, float hiz, float& t_enter)
+{
+    float ax, bx, ay, by, az, bz;
+    plane_pair_fma(lox, hix, r.inv_min[0], r.inv_max[0], ax, bx);
+    plane_pair_fma(loy, hiy, r.inv_min[1], r.inv_max[1], ay, by);
+    plane_pair_fma(loz, hiz, r.inv_min[2], r.inv_max[2], az, bz);
+    const float tn = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fminf(az, bz));
+    const float tf = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
+    t_enter = tn;
+    return tn <= tf && tf > r.tmin;
+}
+
+// Both child boxes of a binary node (render rays or the exact test).
+template <bool RENDER>
+__device__ __forceinline__ void slab_pair(const TraversalRay& r, float4 bx, float4 by, float4 bz,
+                                          bool& pl, float& tl, bool& pr, float& tr)
+{
+    if (RENDER && LMGPU_RENDER_FMA_SLAB) {
+        pl = slab_render(r, bx.x, bx.y, by.x, by.y, bz.x, bz.y, tl);
+        pr = slab_render(r, bx.z, bx.w, by.z, by.w, bz.z, bz.w, tr);
+    } else if (LMGPU_TRACE_FAST_SLAB && (r.neg & RAY_FINITE_INV)) {
+        pl = slab_finite(r, bx.x, bx.y, by.x, by.y, bz.x, bz.y, tl);
+        pr = slab_finite(r, bx.z, bx.w, by.z, by.w, bz.z, bz.w, tr);
+    } else {
+        pl = slab_intrinsic(r, bx.x, bx.y, by.x, by.y, bz.x, bz.y, tl);
+        pr = slab_intrinsic(r, bx.z, bx.w, by.z, by.w, bz.z, bz.w, tr);
+    }
+}
+
+// One box (the root's) for render rays or the exact test.
+template <bool RENDER>
+__device__ __forceinline__ bool slab_box(const TraversalRay& r, float lox, float hix, float loy, float hiy,
+                                         float loz, float hiz, float& t_enter)
+{
+    if (RENDER && LMGPU_RENDER_FMA_SLAB) return slab_render(r, lox, hix, loy, hiy, loz, hiz, t_enter);
+    return slab_intrinsic(r, lox, hix, loy, hiy, loz, hiz, t_enter);
+}
+
 // TriAccel::Intersect (triaccel.h:100-160) in the reference's order.
 // Returns true on a hit within [mint, maxt]; u, v, t are then valid.
 __device__ __forceinline__ bool triaccel_intersect(const float4 q0, const float4 q1, const float4 q2,
@@ -162,6 +241,34 @@ __device__ __forceinline__ bool triaccel_intersect(const float4 q0, const float4
     return u >= 0.0f && v >= 0.0f && __fadd_rn(u, v) <= 1.0f;
 }
 
+// The same TriAccel test for renders, which need the same expected image,
+// not bit-identical hits: multiply-adds and an approximate division
+// (div.approx: a reciprocal and a multiply) in place of the separately
+// rounded products and the correctly rounded division. Hits may differ
+// from the exact test's only within rounding of the edges and of t.
+__device__ __forceinline__ bool triaccel_intersect_fast(const float4 q0, const float4 q1, const float4 q2,
+                                                        const TraversalRay& r, float maxt,
+                                                        float& u, float& v, float& t)
+{
+    const uint32_t k = __float_as_uint(q0.x) & TRI_AXIS_MASK;
+    if (k == 3u) return false;
+    const float o_u = k == 0 ? r.o[1] : (k == 1 ? r.o[2] : r.o[0]);
+    const float o_v = k == 0 ? r.o[2] : (k == 1 ? r.o[0] : r.o[1]);
+    const float o_k = k == 0 ? r.o[0] : (k == 1 ? r.o[1] : r.o[2]);
+    const float d_u = k == 0 ? r.d[1] : (k == 1 ? r.d[2] : r.d[0]);
+    const float d_v = k == 0 ? r.d[2] : (k == 1 ? r.d[0] : r.d[1]);
+    const float d_k = k == 0 ? r.d[0] : (k == 1 ? r.d[1] : r.d[2]);
+    const float num = __fmaf_rn(-o_v, q0.z, __fmaf_rn(-o_u, q0.y, q0.w)) - o_k;
+    const float den = __fmaf_rn(d_v, q0.z, __fmaf_rn(d_u, q0.y, d_k));
+    t = __fdividef(num, den);
+    if (!(t >= r.tmin && t <= maxt)) return false;
+    const float hu = __fmaf_rn(t, d_u, o_u) - q1.x;
+    const float hv = __fmaf_rn(t, d_v, o_v) - q1.y;
+    u = __fmaf_rn(hv, q1.z, hu * q1.w);
+    v = __fmaf_rn(hu, q2.x, hv * q2.y);
+    return u >= 0.0f && v >= 0.0f && u + v <= 1.0f;
+}
+
 struct Hit {
     int32_t tri;   // reference TriAccel index, -1 = miss
     float t, u, v;
@@ -174,7 +281,12 @@ struct TraceStats {
 
 // Leaf loop: every record of the leaf is tested against the running maxT;
 // a hit sets maxT = t so later records need t <= new maxT (scene.bvh.cpp:416-427).
-template <bool ANY_HIT>
+// FAST selects triaccel_intersect_fast (render rays); otherwise the
+// reference's exact test.
+#ifndef LMGPU_RENDER_FAST_TRI
+#define LMGPU_RENDER_FAST_TRI 1
+#endif
+template <bool ANY_HIT, bool FAST = false>
 __device__ __forceinline__ bool trace_leaf(const TriRecord* __restrict__ tris, int32_t first,
                                            TraversalRay& r, Hit& h, TraceStats* st)
 {
@@ -183,7 +295,8 @@ __device__ __forceinline__ bool trace_leaf(const TriRecord* __restrict__ tris, i
         const float4 q0 = __ldg(p), q1 = __ldg(p + 1), q2 = __ldg(p + 2);
         if (st) st->tris++;
         float u, v, t;
-        if (triaccel_intersect(q0, q1, q2, r, r.tmax, u, v, t)) {
+        if ((FAST && LMGPU_RENDER_FAST_TRI) ? triaccel_intersect_fast(q0, q1, q2, r, r.tmax, u, v, t)
+                                            : triaccel_intersect(q0, q1, q2, r, r.tmax, u, v, t)) {
             r.tmax = t;
             h.tri = static_cast<int32_t>(__float_as_uint(q2.z));
             h.t = t; h.u = u; h.v = v;
@@ -242,13 +355,14 @@ __device__ __forceinline__ void pop_next(TravState& ts, Stack stack, const Trave
 }
 
 // Root box test (the reference tests every node's own box on entry).
+template <bool RENDER = false>
 __device__ __forceinline__ void trav_begin(TravState& ts, int32_t root_ref, const float* root_box,
                                            const TraversalRay& r, TraceStats* st)
 {
     ts.sp = 0;
     float te;
     if (st) st->nodes++;
-    ts.ref = (slab_intrinsic(r, root_box[0], root_box[3], root_box[1], root_box[4], root_box[2], root_box[5], te) &&
+    ts.ref = (slab_box<RENDER>(r, root_box[0], root_box[3], root_box[1], root_box[4], root_box[2], root_box[5], te) &&
               te < r.tmax) ? root_ref : REF_DONE;
 }
 
@@ -257,7 +371,7 @@ __device__ __forceinline__ void trav_begin(TravState& ts, int32_t root_ref, cons
 // `may_exit`, it also returns (state intact, at an internal node) once fewer
 // than EXIT_BELOW lanes of the warp are still descending, after at least one
 // step: the caller resumes it later, so the ray's walk is unchanged.
-template <int EXIT_BELOW = 0, class Stack>
+template <int EXIT_BELOW = 0, bool RENDER = false, class Stack>
 __device__ __forceinline__ bool bvh2_descend(const Bvh2Node* __restrict__ nodes, TravState& ts, Stack stack,
                                              int stack_cap, const TraversalRay& r, TraceStats* st,
                                              bool may_exit = false)
@@ -271,13 +385,7 @@ __device__ __forceinline__ bool bvh2_descend(const Bvh2Node* __restrict__ nodes,
         const int4 meta = __ldg(reinterpret_cast<const int4*>(np + 3));
         float tl = 0.f, tr = 0.f;
         bool pl, pr;
-        if (LMGPU_TRACE_FAST_SLAB && (r.neg & RAY_FINITE_INV)) {
-            pl = slab_finite(r, bx.x, bx.y, by.x, by.y, bz.x, bz.y, tl);
-            pr = slab_finite(r, bx.z, bx.w, by.z, by.w, bz.z, bz.w, tr);
-        } else {
-            pl = slab_intrinsic(r, bx.x, bx.y, by.x, by.y, bz.x, bz.y, tl);
-            pr = slab_intrinsic(r, bx.z, bx.w, by.z, by.w, bz.z, bz.w, tr);
-        }
+        slab_pair<RENDER>(r, bx, by, bz, pl, tl, pr, tr);
         const bool right_first = (r.neg >> meta.z) & 1u;
         const int32_t near_ref = right_first ? meta.y : meta.x;
         const int32_t far_ref = right_first ? meta.x : meta.y;
@@ -306,7 +414,8 @@ __device__ __forceinline__ bool bvh2_descend(const Bvh2Node* __restrict__ nodes,
 // Closest hit (or any hit) through the binary children-in-parent BVH.
 // `stack` is per-thread scratch of `stack_cap` (ref, t_enter) pairs.
 // Returns false if the stack bound was exceeded (the caller flags an error).
-template <bool ANY_HIT>
+// RENDER: a render ray (setup_ray<true>) with the renders' arithmetic.
+template <bool ANY_HIT, bool RENDER = false>
 __device__ __forceinline__ bool trace_bvh2(const Bvh2Node* __restrict__ nodes,
                                            const TriRecord* __restrict__ tris,
                                            int32_t root_ref, const float* root_box,
@@ -315,12 +424,101 @@ __device__ __forceinline__ bool trace_bvh2(const Bvh2Node* __restrict__ nodes,
 {
     h.tri = -1;
     TravState ts;
-    trav_begin(ts, root_ref, root_box, r, st);
+    trav_begin<RENDER>(ts, root_ref, root_box, r, st);
     for (;;) {
-        if (!bvh2_descend(nodes, ts, stack, stack_cap, r, st)) return false;
+        if (!bvh2_descend<0, RENDER>(nodes, ts, stack, stack_cap, r, st)) return false;
         if (ts.ref == REF_DONE) return true;
-        if (trace_leaf<ANY_HIT>(tris, ~ts.ref, r, h, st) && ANY_HIT) return true;
+        if (trace_leaf<ANY_HIT, RENDER>(tris, ~ts.ref, r, h, st) && ANY_HIT) return true;
         pop_next(ts, stack, r, st);
+    }
+}
+
+// ---------------------------------------------------------------- any hit
+// Visibility queries (shadow rays) stop at their first hit, so their maxT
+// never changes while they walk: a far child can be tested against maxT
+// when it is pushed instead of when it is popped. The stack then holds
+// node references only (4 bytes), and a pop needs no test. Every box test
+// uses the same arithmetic and the same maxT as the closest-hit walk's, so
+// the walk reaches a hit exactly when the closest-hit walk would find one:
+// the visibility verdict is the same.
+#ifndef LMGPU_TRACE_ANYHIT_WALK
+#define LMGPU_TRACE_ANYHIT_WALK 1     // 0: visibility queries take the closest-hit walk
+#endif
+__device__ __forceinline__ void ref_put(int* s, int i, int v) { s[i] = v; }
+__device__ __forceinline__ int ref_get(const int* s, int i) { return s[i]; }
+
+template <int S>
+struct SplitRefStack {
+    int (*sh)[128];
+    int* local;
+};
+template <int S>
+__device__ __forceinline__ void ref_put(const SplitRefStack<S>& s, int i, int v)
+{
+    if (i < S) s.sh[i][threadIdx.x] = v;
+    else s.local[i - S] = v;
+}
+template <int S>
+__device__ __forceinline__ int ref_get(const SplitRefStack<S>& s, int i)
+{
+    return i < S ? s.sh[i][threadIdx.x] : s.local[i - S];
+}
+
+template <class Stack>
+__device__ __forceinline__ void pop_any(TravState& ts, Stack stack)
+{
+    ts.ref = ts.sp > 0 ? ref_get(stack, --ts.sp) : REF_DONE;
+}
+
+// Any-hit descent through the binary nodes (visit order as bvh2_descend:
+// the right child first iff the ray direction is negative on the split
+// axis). Returns false on stack overflow; EXIT_BELOW / may_exit as there.
+template <int EXIT_BELOW = 0, bool RENDER = false, class Stack>
+__device__ __forceinline__ bool bvh2_descend_any(const Bvh2Node* __restrict__ nodes, TravState& ts, Stack stack,
+                                                 int stack_cap, const TraversalRay& r, TraceStats* st,
+                                                 bool may_exit = false)
+{
+    bool stepped = false;
+    while (ts.ref >= 0 && ts.ref != REF_DONE) {
+        if (EXIT_BELOW > 0 && may_exit && stepped && __popc(__activemask()) < EXIT_BELOW) break;
+        stepped = true;
+        const float4* np = reinterpret_cast<const float4*>(nodes + ts.ref);
+        const float4 bx = __ldg(np), by = __ldg(np + 1), bz = __ldg(np + 2);
+        const int4 meta = __ldg(reinterpret_cast<const int4*>(np + 3));
+        float tl = 0.f, tr = 0.f;
+        bool pl, pr;
+        slab_pair<RENDER>(r, bx, by, bz, pl, tl, pr, tr);
+        if (st) st->nodes += 2;
+        const bool hl = pl && tl < r.tmax, hr = pr && tr < r.tmax;
+        if (hl && hr) {
+            const bool right_first = (r.neg >> meta.z) & 1u;
+            if (ts.sp >= stack_cap) return false;
+            ref_put(stack, ts.sp++, right_first ? meta.x : meta.y);
+            ts.ref = right_first ? meta.y : meta.x;
+        } else if (hl || hr) {
+            ts.ref = hl ? meta.x : meta.y;
+        } else {
+            pop_any(ts, stack);
+        }
+    }
+    return true;
+}
+
+// Any hit through the binary nodes with a per-thread reference stack of
+// `stack_cap` entries; h.tri >= 0 iff some triangle is hit in [tmin, tmax].
+template <bool RENDER>
+__device__ __forceinline__ bool trace_bvh2_any(const Bvh2Node* __restrict__ nodes, const TriRecord* __restrict__ tris,
+                                               int32_t root_ref, const float* root_box, TraversalRay& r, Hit& h,
+                                               int* stack, int stack_cap, TraceStats* st)
+{
+    h.tri = -1;
+    TravState ts;
+    trav_begin<RENDER>(ts, root_ref, root_box, r, st);
+    for (;;) {
+        if (!bvh2_descend_any<0, RENDER>(nodes, ts, stack, stack_cap, r, st)) return false;
+        if (ts.ref == REF_DONE) return true;
+        if (trace_leaf<true, RENDER>(tris, ~ts.ref, r, h, st)) return true;
+        pop_any(ts, stack);
     }
 }
 

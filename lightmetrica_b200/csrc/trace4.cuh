@@ -15,7 +15,7 @@ namespace lmgpu {
 
 // 4-wide nodes: descends until the state reaches a leaf or finishes.
 // Returns false on stack overflow. EXIT_BELOW / may_exit as in bvh2_descend.
-template <int EXIT_BELOW = 0, class Stack>
+template <int EXIT_BELOW = 0, bool RENDER = false, class Stack>
 __device__ __forceinline__ bool bvh4_descend(const Bvh4Node* __restrict__ nodes, TravState& ts, Stack stack,
                                              int stack_cap, const TraversalRay& r, TraceStats* st,
                                              bool may_exit = false)
@@ -31,10 +31,13 @@ __device__ __forceinline__ bool bvh4_descend(const Bvh4Node* __restrict__ nodes,
         const int4 child = __ldg(reinterpret_cast<const int4*>(np + 6));
         const int4 axes = __ldg(reinterpret_cast<const int4*>(np + 7));
         float t0 = 0.f, t1 = 0.f, t2 = 0.f, t3 = 0.f;
-        const bool p0 = slab_intrinsic(r, lox.x, hix.x, loy.x, hiy.x, loz.x, hiz.x, t0);
-        const bool p1 = slab_intrinsic(r, lox.y, hix.y, loy.y, hiy.y, loz.y, hiz.y, t1);
-        const bool p2 = slab_intrinsic(r, lox.z, hix.z, loy.z, hiy.z, loz.z, hiz.z, t2);
-        const bool p3 = slab_intrinsic(r, lox.w, hix.w, loy.w, hiy.w, loz.w, hiz.w, t3);
+        // Empty slots hold lo > hi on every axis, which the exact test
+        // rejects; the render test's min/max form does not, so their
+        // reference (BVH4_EMPTY) excludes them below.
+        const bool p0 = slab_box<RENDER>(r, lox.x, hix.x, loy.x, hiy.x, loz.x, hiz.x, t0);
+        const bool p1 = slab_box<RENDER>(r, lox.y, hix.y, loy.y, hiy.y, loz.y, hiz.y, t1);
+        const bool p2 = slab_box<RENDER>(r, lox.z, hix.z, loy.z, hiy.z, loz.z, hiz.z, t2);
+        const bool p3 = slab_box<RENDER>(r, lox.w, hix.w, loy.w, hiy.w, loz.w, hiz.w, t3);
         if (st) st->nodes += 4;
         // Visit order, 4 bits per slot.
         uint32_t order = 0;
@@ -65,7 +68,7 @@ __device__ __forceinline__ bool bvh4_descend(const Bvh4Node* __restrict__ nodes,
                 const bool ps = sl == 0 ? p0 : sl == 1 ? p1 : sl == 2 ? p2 : p3;
                 const float tt = sl == 0 ? t0 : sl == 1 ? t1 : sl == 2 ? t2 : t3;
                 const int32_t cr = sl == 0 ? child.x : sl == 1 ? child.y : sl == 2 ? child.z : child.w;
-                if (ps) { refs[np_] = cr; ts4[np_] = tt; np_++; }
+                if (ps && cr != BVH4_EMPTY) { refs[np_] = cr; ts4[np_] = tt; np_++; }
             }
         }
         int first = -1;
@@ -85,7 +88,7 @@ __device__ __forceinline__ bool bvh4_descend(const Bvh4Node* __restrict__ nodes,
     return true;
 }
 
-template <bool ANY_HIT>
+template <bool ANY_HIT, bool RENDER = false>
 __device__ __forceinline__ bool trace_bvh4(const Bvh4Node* __restrict__ nodes,
                                            const TriRecord* __restrict__ tris,
                                            int32_t root_ref, const float* root_box,
@@ -94,11 +97,11 @@ __device__ __forceinline__ bool trace_bvh4(const Bvh4Node* __restrict__ nodes,
 {
     h.tri = -1;
     TravState ts;
-    trav_begin(ts, root_ref, root_box, r, st);
+    trav_begin<RENDER>(ts, root_ref, root_box, r, st);
     for (;;) {
-        if (!bvh4_descend(nodes, ts, stack, stack_cap, r, st)) return false;
+        if (!bvh4_descend<0, RENDER>(nodes, ts, stack, stack_cap, r, st)) return false;
         if (ts.ref == REF_DONE) return true;
-        if (trace_leaf<ANY_HIT>(tris, ~ts.ref, r, h, st) && ANY_HIT) return true;
+        if (trace_leaf<ANY_HIT, RENDER>(tris, ~ts.ref, r, h, st) && ANY_HIT) return true;
         pop_next(ts, stack, r, nullptr);
     }
 }

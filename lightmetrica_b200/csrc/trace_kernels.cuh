@@ -61,6 +61,14 @@ struct min_blocks
 template <class IO>
 struct min_blocks<IO, std::void_t<decltype(IO::MIN_BLOCKS)>> : std::integral_constant<int, IO::MIN_BLOCKS> {};
 
+// Render rays (the path tracer's queues) declare RENDER = true: their
+// triangle tests take triaccel_intersect_fast; the intersection API keeps
+// the reference's exact arithmetic.
+template <class IO, class = void>
+struct render_rays : std::false_type {};
+template <class IO>
+struct render_rays<IO, std::void_t<decltype(IO::RENDER)>> : std::bool_constant<IO::RENDER> {};
+
 // Pause threshold of a descent: an I/O policy may declare EXIT_BELOW.
 template <class IO, class = void>
 struct exit_below : std::integral_constant<int, LMGPU_TRACE_EXIT_BELOW> {};
@@ -75,12 +83,12 @@ struct LaneScene {
 };
 
 
-template <int LAYOUT, int EXIT, class Stack>
+template <int LAYOUT, int EXIT, bool RENDER, class Stack>
 __device__ __forceinline__ bool descend(const LaneScene& s, TravState& ts, Stack stack, int cap,
                                         const TraversalRay& r, bool may_exit, TraceStats* st)
 {
-    if (LAYOUT == LMGPU_LAYOUT_BVH2) return bvh2_descend<EXIT>(s.bvh2, ts, stack, cap, r, st, may_exit);
-    return bvh4_descend<EXIT>(s.bvh4, ts, stack, cap, r, st, may_exit);
+    if (LAYOUT == LMGPU_LAYOUT_BVH2) return bvh2_descend<EXIT, RENDER>(s.bvh2, ts, stack, cap, r, st, may_exit);
+    return bvh4_descend<EXIT, RENDER>(s.bvh4, ts, stack, cap, r, st, may_exit);
 }
 
 // Adds each lane's counts to counts[0] (binary-node slab tests; four per
@@ -111,19 +119,32 @@ __device__ __forceinline__ void add_trace_stats(const TraceStats& st, unsigned l
 // The COUNT instantiation (measurement runs only) also adds the rays' slab
 // and TriAccel tests to counts[0..1]; the walk is the same. The stack bound
 // is the scene's stack_cap where that is below STACK.
+// Shadow rays through binary nodes take the any-hit walk (bvh2_descend_any:
+// a stack of node references, no pop-time tests), whose visibility verdicts
+// equal the closest-hit walk's.
+template <int LAYOUT, bool ANY_HIT>
+struct RefStackWalk : std::bool_constant<LMGPU_TRACE_ANYHIT_WALK && ANY_HIT && LAYOUT == LMGPU_LAYOUT_BVH2> {};
+
 template <int LAYOUT, int STACK, bool ANY_HIT, class IO, bool COUNT = false>
 __global__ void __launch_bounds__(128, min_blocks<IO>::value)
 k_trace_persistent(const DeviceScene s, const IO io, int32_t* status, unsigned long long* next_ray,
                    unsigned long long* counts)
 {
     constexpr unsigned FULL = 0xffffffffu;
+    constexpr bool REFS = RefStackWalk<LAYOUT, ANY_HIT>::value;
+    constexpr bool RENDER = render_rays<IO>::value;
 #if LMGPU_TRACE_SHARED_STACK > 0
-    constexpr int SH = LMGPU_TRACE_SHARED_STACK < STACK ? LMGPU_TRACE_SHARED_STACK : STACK;
-    __shared__ int2 stack_sh[SH][128];
-    int2 stack_local[STACK > SH ? STACK - SH : 1];
-    const SplitStack<SH> stack{ stack_sh, stack_local };
+    // The shared part takes the same bytes either way: twice as many
+    // 4-byte references as (reference, entry distance) pairs.
+    constexpr int SH0 = REFS ? 2 * LMGPU_TRACE_SHARED_STACK : LMGPU_TRACE_SHARED_STACK;
+    constexpr int SH = SH0 < STACK ? SH0 : STACK;
+    using Entry = std::conditional_t<REFS, int, int2>;
+    __shared__ Entry stack_sh[SH][128];
+    Entry stack_local[STACK > SH ? STACK - SH : 1];
+    using StackT = std::conditional_t<REFS, SplitRefStack<SH>, SplitStack<SH>>;
+    const StackT stack{ stack_sh, stack_local };
 #else
-    int2 stack[STACK];
+    std::conditional_t<REFS, int, int2> stack[STACK];
 #endif
     const int64_t n = io.count();
     const unsigned lane = threadIdx.x & 31u;
@@ -152,7 +173,7 @@ k_trace_persistent(const DeviceScene s, const IO io, int32_t* status, unsigned l
             if (idle) {
                 idx = (int64_t)base + __popc(need & ((1u << lane) - 1u));
                 if (idx < n) {
-                    setup_ray(r, io.load(idx));
+                    setup_ray<RENDER>(r, io.load(idx));
                     h.tri = -1;
                     if constexpr (per_ray_scene<IO>::value) {
                         const DeviceScene& rs = io.ray_scene(idx);
@@ -160,9 +181,9 @@ k_trace_persistent(const DeviceScene s, const IO io, int32_t* status, unsigned l
                         ls.bvh4 = rs.bvh4;
                         ls.tris = rs.tris;
                         if (rs.num_tris > 0)
-                            trav_begin(ts, LAYOUT == LMGPU_LAYOUT_BVH2 ? rs.root_ref : rs.root_ref4, rs.root_box, r, st);
+                            trav_begin<RENDER>(ts, LAYOUT == LMGPU_LAYOUT_BVH2 ? rs.root_ref : rs.root_ref4, rs.root_box, r, st);
                     } else {
-                        trav_begin(ts, root, s.root_box, r, st);
+                        trav_begin<RENDER>(ts, root, s.root_box, r, st);
                     }
                     if (ts.ref == REF_DONE) io.store(idx, h, r);
                 }
@@ -171,14 +192,18 @@ k_trace_persistent(const DeviceScene s, const IO io, int32_t* status, unsigned l
             break;
         }
         if (ts.ref != REF_DONE) {
-            if (!descend<LAYOUT, exit_below<IO>::value>(ls, ts, stack, cap, r, !exhausted, st)) {
+            bool ok;
+            if constexpr (REFS) ok = bvh2_descend_any<exit_below<IO>::value, RENDER>(ls.bvh2, ts, stack, cap, r, st, !exhausted);
+            else ok = descend<LAYOUT, exit_below<IO>::value, RENDER>(ls, ts, stack, cap, r, !exhausted, st);
+            if (!ok) {
                 atomicOr(status, STATUS_STACK_OVERFLOW);
                 h.tri = -1;
                 ts.ref = REF_DONE;
             } else if (ts.ref < 0) {           // at a leaf (a paused descent resumes next round)
                 // (a binary pop is the reference's far-child test; 4-wide
                 // nodes count their four slab tests when fetched)
-                if (trace_leaf<ANY_HIT>(ls.tris, ~ts.ref, r, h, st) && ANY_HIT) ts.ref = REF_DONE;
+                if (trace_leaf<ANY_HIT, RENDER>(ls.tris, ~ts.ref, r, h, st) && ANY_HIT) ts.ref = REF_DONE;
+                else if constexpr (REFS) pop_any(ts, stack);
                 else pop_next(ts, stack, r, LAYOUT == LMGPU_LAYOUT_BVH2 ? st : nullptr);
             }
             if (ts.ref == REF_DONE) io.store(idx, h, r);
@@ -215,10 +240,9 @@ int resident_blocks(K kernel)
 // the naive layout. `max_rays` bounds the grid (0 = resident grid). COUNT
 // launches the counting instantiation, adding to `counts` (BVH layouts).
 template <bool ANY_HIT, int STACK, bool COUNT, class IO>
-int launch_trace_stack(LmgpuScene* sc, const IO& io, int64_t max_rays, cudaStream_t stream,
+int launch_trace_stack(LmgpuScene* sc, const DeviceScene& s, const IO& io, int64_t max_rays, cudaStream_t stream,
                        unsigned long long* counts)
 {
-    const DeviceScene& s = sc->dev;
     if (s.layout == LMGPU_LAYOUT_NAIVE || s.num_tris == 0) {
         if (COUNT) return fail(LMGPU_ERR_UNSUPPORTED, "traversal counters need a BVH layout");
         const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((max_rays + 127) / 128, 148 * 64));
@@ -245,15 +269,18 @@ int launch_trace_stack(LmgpuScene* sc, const IO& io, int64_t max_rays, cudaStrea
     return LMGPU_OK;
 }
 
+// `render` traces the scene's render view (its render tree), else the
+// reference's tree.
 template <bool ANY_HIT, class IO, bool COUNT = false>
 int launch_trace(LmgpuScene* sc, const IO& io, int64_t max_rays, cudaStream_t stream,
-                 unsigned long long* counts = nullptr)
+                 unsigned long long* counts = nullptr, bool render = false)
 {
-    const int cap = sc->dev.stack_cap;
-    if (cap <= 32) return launch_trace_stack<ANY_HIT, 32, COUNT>(sc, io, max_rays, stream, counts);
-    if (cap <= 64) return launch_trace_stack<ANY_HIT, 64, COUNT>(sc, io, max_rays, stream, counts);
-    if (cap <= 128) return launch_trace_stack<ANY_HIT, 128, COUNT>(sc, io, max_rays, stream, counts);
-    if (cap <= 256) return launch_trace_stack<ANY_HIT, 256, COUNT>(sc, io, max_rays, stream, counts);
+    const DeviceScene& s = render ? sc->rdev : sc->dev;
+    const int cap = s.stack_cap;
+    if (cap <= 32) return launch_trace_stack<ANY_HIT, 32, COUNT>(sc, s, io, max_rays, stream, counts);
+    if (cap <= 64) return launch_trace_stack<ANY_HIT, 64, COUNT>(sc, s, io, max_rays, stream, counts);
+    if (cap <= 128) return launch_trace_stack<ANY_HIT, 128, COUNT>(sc, s, io, max_rays, stream, counts);
+    if (cap <= 256) return launch_trace_stack<ANY_HIT, 256, COUNT>(sc, s, io, max_rays, stream, counts);
     return fail(LMGPU_ERR_UNSUPPORTED, "BVH deeper than the largest compiled traversal stack (256)");
 }
 

@@ -36,6 +36,7 @@ STATUS_NAMES = {OK: "OK", ERR_INVALID: "INVALID", ERR_OOM: "OOM", ERR_CUDA: "CUD
                 ERR_TIMEOUT: "TIMEOUT", ERR_UNSUPPORTED: "UNSUPPORTED"}
 
 LAYOUT_BVH2, LAYOUT_BVH4, LAYOUT_NAIVE = 0, 1, 2
+RENDER_TREE_SAH, RENDER_TREE_REFERENCE = 0, 1
 BSDF_DIFFUSE, BSDF_MIRROR, BSDF_DIFFUSE_MIRROR, BSDF_BLACK = 0, 1, 2, 3
 RENDER_PT, RENDER_PT_DIRECT, RENDER_PT_MIS = 0, 1, 2
 SAMPLING_STRATIFIED, SAMPLING_UNIFORM = 0, 1
@@ -63,13 +64,16 @@ class SceneDesc(ctypes.Structure):
                 ("has_camera", c_int32), ("camera_eye", c_float * 3), ("camera_center", c_float * 3),
                 ("camera_up", c_float * 3), ("camera_fovy_degrees", c_float),
                 ("film_width", c_int32), ("film_height", c_int32),
-                ("layout", c_int32), ("build_threads", c_int32), ("max_stack_entries", c_int32)]
+                ("layout", c_int32), ("build_threads", c_int32), ("max_stack_entries", c_int32),
+                ("render_tree", c_int32)]
 
 
 class SceneInfo(ctypes.Structure):
     _fields_ = [("num_triangles", c_int64), ("num_nodes", c_int64), ("num_leaves", c_int64),
                 ("max_depth", c_int32), ("layout", c_int32), ("device_bytes", c_int64),
-                ("build_seconds", c_double), ("bounds_min", c_float * 3), ("bounds_max", c_float * 3)]
+                ("build_seconds", c_double), ("bounds_min", c_float * 3), ("bounds_max", c_float * 3),
+                ("render_tree", c_int32), ("render_max_depth", c_int32), ("render_num_nodes", c_int64),
+                ("render_num_leaves", c_int64), ("render_build_seconds", c_double)]
 
 
 class RaysSoA(ctypes.Structure):

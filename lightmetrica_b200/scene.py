@@ -199,6 +199,7 @@ class Scene:
         self.primitives: Optional[Primitives] = None
         self.build_threads = 0
         self.max_stack_entries = 0
+        self.render_tree = N.RENDER_TREE_SAH
         self.handle = None
         self._keep = []
 
@@ -206,14 +207,20 @@ class Scene:
     def load(self, primitives: Primitives) -> None:
         self.primitives = primitives
 
-    # reference Scene::Configure: the GPU scene reads `build_threads` and
-    # `max_stack_entries` (the traversal stack bound per ray, 0 = automatic).
+    # reference Scene::Configure: the GPU scene reads `build_threads`,
+    # `max_stack_entries` (the traversal stack bound per ray, 0 = automatic)
+    # and `render_tree` ("sah": renders traverse a second tree built for
+    # traversal cost, the default; "reference": the reference's tree).
     def configure(self, node: Optional[dict] = None) -> bool:
         node = node or {}
         self.build_threads = int(node.get("build_threads", 0))
         self.max_stack_entries = int(node.get("max_stack_entries", 0))
         if self.max_stack_entries < 0:
             raise ValueError("max_stack_entries must be >= 0")
+        tree = node.get("render_tree", "sah")
+        if tree not in ("sah", "reference"):
+            raise ValueError("render_tree must be 'sah' or 'reference'")
+        self.render_tree = N.RENDER_TREE_SAH if tree == "sah" else N.RENDER_TREE_REFERENCE
         return True
 
     def build(self) -> bool:
@@ -245,7 +252,10 @@ class Scene:
         return {"num_triangles": inf.num_triangles, "num_nodes": inf.num_nodes, "num_leaves": inf.num_leaves,
                 "max_depth": inf.max_depth, "layout": inf.layout, "device_bytes": inf.device_bytes,
                 "build_seconds": inf.build_seconds,
-                "bounds_min": list(inf.bounds_min), "bounds_max": list(inf.bounds_max)}
+                "bounds_min": list(inf.bounds_min), "bounds_max": list(inf.bounds_max),
+                "render_tree": "sah" if inf.render_tree == N.RENDER_TREE_SAH else "reference",
+                "render_max_depth": inf.render_max_depth, "render_num_nodes": inf.render_num_nodes,
+                "render_num_leaves": inf.render_num_leaves, "render_build_seconds": inf.render_build_seconds}
 
     def get_aabb_triangles(self):
         i = self.info()
@@ -369,6 +379,7 @@ class Scene:
         desc.layout = self.layout
         desc.build_threads = self.build_threads
         desc.max_stack_entries = self.max_stack_entries
+        desc.render_tree = self.render_tree
         keep += [prims, mat_arr, light_arr]
         return desc, keep
 

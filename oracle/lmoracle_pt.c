@@ -31,7 +31,8 @@
 #define INV_PI 0.31830988618379067154
 #define EPS 1e-7             /* Math::Constants::Eps() (double build) */
 #define EPS_LARGE 1e-5       /* Math::Constants::EpsLarge() (double build) */
-#define MAX_VERTS 64
+#define MAX_VERTS 64              /* initial capacity of a path's vertex records */
+#define MAX_PATH_VERTICES 4096    /* the device's bound on replayed surface vertices */
 
 typedef struct { double x, y, z; } v3;
 static inline v3 mk(double x, double y, double z) { v3 r = { x, y, z }; return r; }
@@ -524,17 +525,48 @@ static void teardown(pt_scene* s)
 typedef struct { int pixel; v3 c; int depth; int light; v3 Le; } event_t;
 
 typedef struct {
-    event_t ev[2 * MAX_VERTS + 2];
-    int nev;
-    int vtri[MAX_VERTS];   /* triangle of surface vertex 1..: index i-1 */
-    int nv;
+    event_t* ev;           /* grows as needed */
+    int nev, cap_ev;
+    int* vtri;             /* triangle of surface vertex 1..: index i-1 */
+    int nv, cap_v;
+    int overflow;          /* the path reached MAX_PATH_VERTICES */
 } path_t;
+
+static path_t* path_new(void)
+{
+    path_t* P = (path_t*)calloc(1, sizeof(path_t));
+    P->cap_ev = 2 * MAX_VERTS + 2;
+    P->cap_v = MAX_VERTS;
+    P->ev = (event_t*)malloc(sizeof(event_t) * P->cap_ev);
+    P->vtri = (int*)malloc(sizeof(int) * P->cap_v);
+    return P;
+}
+
+static void path_free(path_t* P)
+{
+    free(P->ev);
+    free(P->vtri);
+    free(P);
+}
 
 static void add_event(path_t* P, int pixel, v3 c, int depth, int light, v3 Le)
 {
-    if (pixel < 0 || is_zero(c) || P->nev >= 2 * MAX_VERTS + 2) return;
+    if (pixel < 0 || is_zero(c)) return;
+    if (P->nev == P->cap_ev) {
+        P->cap_ev *= 2;
+        P->ev = (event_t*)realloc(P->ev, sizeof(event_t) * P->cap_ev);
+    }
     event_t* e = &P->ev[P->nev++];
     e->pixel = pixel; e->c = c; e->depth = depth; e->light = light; e->Le = Le;
+}
+
+static void add_vertex(path_t* P, int tri)
+{
+    if (P->nv == P->cap_v) {
+        P->cap_v *= 2;
+        P->vtri = (int*)realloc(P->vtri, sizeof(int) * P->cap_v);
+    }
+    P->vtri[P->nv++] = tri;
 }
 
 static void run_sample(const pt_scene* s, uint64_t sample, path_t* P)
@@ -545,6 +577,7 @@ static void run_sample(const pt_scene* s, uint64_t sample, path_t* P)
     uint64_t key = sample_key(d->seed, sample);
     P->nev = 0;
     P->nv = 0;
+    P->overflow = 0;
     double rx, ry;
     double u0 = rnd(key, 0), u1 = rnd(key, 1);
     int64_t pixels = (int64_t)d->width * d->height;
@@ -623,7 +656,11 @@ static void run_sample(const pt_scene* s, uint64_t sample, path_t* P)
             }
             m = tri_material(s, tri);
             surface = 1;
-            if (P->nv < MAX_VERTS) P->vtri[P->nv++] = tri;
+            /* The device replays at most MAX_PATH_VERTICES surface vertices
+             * (paths that long occur only in closed scenes without Russian
+             * roulette, where the reference's loop does not end). */
+            if (P->nv == MAX_PATH_VERTICES) { P->overflow = 1; return; }
+            add_vertex(P, tri);
         }
         int depth_here = P->nv - (surface ? 1 : 0);   /* BSDF factors in thr */
         if (!is_zero(Le)) {
@@ -683,7 +720,7 @@ int64_t orc_render(const orc_pt_desc* d, double* film)
 {
     pt_scene s;
     if (!setup(&s, d)) { teardown(&s); return -1; }
-    path_t* P = (path_t*)malloc(sizeof(path_t));
+    path_t* P = path_new();
     for (int64_t smp = d->sample_begin; smp < d->sample_end; smp++) {
         run_sample(&s, (uint64_t)smp, P);
         for (int e = 0; e < P->nev; e++) {
@@ -692,7 +729,7 @@ int64_t orc_render(const orc_pt_desc* d, double* film)
             film[3 * P->ev[e].pixel + 2] += P->ev[e].c.z;
         }
     }
-    free(P);
+    path_free(P);
     teardown(&s);
     return d->sample_end - d->sample_begin;
 }
@@ -713,7 +750,7 @@ int64_t orc_render_grad(const orc_pt_desc* d, const double* dL_dI, double* d_alb
 {
     pt_scene s;
     if (!setup(&s, d)) { teardown(&s); return -1; }
-    path_t* P = (path_t*)malloc(sizeof(path_t));
+    path_t* P = path_new();
     for (int64_t smp = d->sample_begin; smp < d->sample_end; smp++) {
         run_sample(&s, (uint64_t)smp, P);
         for (int e = 0; e < P->nev; e++) {
@@ -736,7 +773,7 @@ int64_t orc_render_grad(const orc_pt_desc* d, const double* dL_dI, double* d_alb
                 }
         }
     }
-    free(P);
+    path_free(P);
     teardown(&s);
     return d->sample_end - d->sample_begin;
 }

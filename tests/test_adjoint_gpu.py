@@ -214,3 +214,115 @@ def test_c4_scene_gradient_matches_fp64_oracle_and_fd(cuda):
         fd = (loss(alb0, lp) - loss(alb0, lm)) / (float(lp[0, c]) - float(lm[0, c]))
         print(f"emission ch{c}: fd {fd:.6e} adjoint {de[0, c]:.6e}")
         assert abs(de[0, c] - fd) <= 1e-2 * abs(fd)
+
+
+def closed_box(width, height, light_absorbs=True):
+    """The Cornell box closed by a front wall and seen from inside it: a
+    perfect-mirror back wall and tall box, a diffuse-mirror short box, highly
+    reflective diffuse walls (0.95; red and green side walls). With the
+    light's black BSDF its only exit is the light, which takes ~1% of the
+    bounces: without Russian roulette paths run for about a hundred vertices.
+    With `light_absorbs` False the light reflects too and no path ends."""
+    from lightmetrica_b200.scene import (AreaLight, DiffuseBSDF, DiffuseMirrorBSDF, HDRBitmapFilm,
+                                         PerfectMirrorBSDF, PerspectiveCamera, Primitive, Primitives)
+    from lightmetrica_b200.scenes import _box, _mesh, _quad
+    white, red, green = DiffuseBSDF((0.95, 0.95, 0.95)), DiffuseBSDF((0.95, 0.6, 0.5)), DiffuseBSDF((0.5, 0.95, 0.6))
+    prims = Primitives()
+    prims.add(Primitive(mesh=_mesh([_quad((0, 0, 0), (1, 0, 0), (1, 0, 1), (0, 0, 1), (0, 1, 0)),
+                                    _quad((0, 1, 0), (1, 1, 0), (1, 1, 1), (0, 1, 1), (0, -1, 0)),
+                                    _quad((0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1), (0, 0, -1))]), bsdf=white))
+    prims.add(Primitive(mesh=_mesh([_quad((0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1))]),
+                        bsdf=PerfectMirrorBSDF((0.98, 0.98, 0.98))))
+    prims.add(Primitive(mesh=_mesh([_quad((0, 0, 0), (0, 1, 0), (0, 1, 1), (0, 0, 1), (1, 0, 0))]), bsdf=red))
+    prims.add(Primitive(mesh=_mesh([_quad((1, 0, 0), (1, 1, 0), (1, 1, 1), (1, 0, 1), (-1, 0, 0))]), bsdf=green))
+    prims.add(Primitive(mesh=_box((0.33, 0.0, 0.62), (0.30, 0.30, 0.30), -17.0),
+                        bsdf=DiffuseMirrorBSDF((0.9, 0.85, 0.8))))
+    prims.add(Primitive(mesh=_box((0.68, 0.0, 0.35), (0.30, 0.60, 0.30), 17.0),
+                        bsdf=PerfectMirrorBSDF((0.98, 0.98, 0.98))))
+    y = 1.0 - 1e-3
+    prims.add(Primitive(mesh=_mesh([_quad((0.37, y, 0.40), (0.63, y, 0.40), (0.63, y, 0.60), (0.37, y, 0.60),
+                                          (0, -1, 0))]),
+                        bsdf=DiffuseBSDF((0.0, 0.0, 0.0) if light_absorbs else (0.9, 0.9, 0.9)),
+                        light=AreaLight((17.0, 12.0, 4.0))))
+    prims.camera = PerspectiveCamera(fovy=70.0, eye=(0.5, 0.5, 0.97), center=(0.5, 0.45, 0.0), up=(0, 1, 0),
+                                     film=HDRBitmapFilm(width, height))
+    return prims
+
+
+def test_long_paths_gradient_matches_fp64_oracle(cuda):
+    """Unbounded depth (max_path_vertices = -1) and no Russian roulette in
+    the closed mirror-and-diffuse box: paths run for hundreds of vertices.
+    The adjoint keeps records for the first 32 vertices and replays deeper
+    tails from a checkpoint; its albedo and emission gradients must equal
+    the oracle's FP64 gradient on the same random numbers, and its forward
+    image the wavefront renderer's image of the same samples."""
+    import torch
+    from lightmetrica_b200 import create_scheduler
+    W = H = 24
+    spp = 8
+    prims = closed_box(W, H)
+    scene = create_scene("bvh")
+    scene.load(prims)
+    scene.configure({})
+    scene.build()
+    r = create_renderer("pt.mis")
+    r.configure({"rr_depth": -1, "max_path_vertices": -1, "sampler": {"rng_seed": 21}})
+    sched = create_scheduler("mt")
+    sched.configure({"num_samples": W * H * spp, "film_fp64": True})
+    film = sched.render(r, scene)
+    deepest = sched.last_stats["max_bounces_run"]
+    print(f"deepest bounce: {deepest}")
+    assert deepest > 100
+    dr = DifferentiableRender(scene, r, W * H * spp)
+    alb0 = triangle_albedo(prims)
+    em0 = light_emission(prims)
+    alb, em = torch.from_numpy(alb0).to(cuda), torch.from_numpy(em0).to(cuda)
+    img = dr.forward(alb, em)
+    np.testing.assert_allclose(img.cpu().numpy(), film, rtol=1e-3, atol=1e-5)
+    target = dr.forward(torch.from_numpy((alb0 * 0.9).astype(np.float32)).to(cuda), em)
+    dL = 2.0 * (img - target)
+    da, de = dr.backward(alb, em, dL)
+    ga, gl = oracle.oracle_grad(prims, dL.cpu().numpy(), "pt.mis", spp=spp, rr_depth=-1, max_path_vertices=-1,
+                                seed=21, tri_albedo=alb0, threads=os.cpu_count() or 1)
+    da = da.cpu().numpy()
+    rel = np.linalg.norm(da - ga) / np.linalg.norm(ga)
+    print(f"long paths: |d_albedo - fp64| / |fp64| = {rel:.2e}")
+    assert rel <= 1e-2
+    np.testing.assert_allclose(de.cpu().numpy(), gl, rtol=1e-2)
+    # Vertices beyond the recorded 32 carry a real share of the gradient:
+    # truncating the paths there changes it.
+    r33 = create_renderer("pt.mis")
+    r33.configure({"rr_depth": -1, "max_path_vertices": 34, "sampler": {"rng_seed": 21}})
+    da33, _ = DifferentiableRender(scene, r33, W * H * spp).backward(alb, em, dL)
+    assert np.linalg.norm(da33.cpu().numpy() - da) > 0.05 * np.linalg.norm(da)
+    scene.close()
+
+
+def test_replay_bound_overflow_is_reported(cuda):
+    """A closed box whose light reflects too: without Russian roulette no
+    path ends (nor would the reference's loop). The replay stops at its
+    bound of 4096 surface vertices, raises the status word, and both passes
+    report LMGPU_ERR_QUEUE_OVERFLOW; with a depth bound the same scene then
+    renders."""
+    import torch
+    from lightmetrica_b200 import native
+    prims = closed_box(8, 8, light_absorbs=False)
+    scene = create_scene("bvh")
+    scene.load(prims)
+    scene.configure({})
+    scene.build()
+    r = create_renderer("pt.mis")
+    r.configure({"rr_depth": -1, "max_path_vertices": -1, "sampler": {"rng_seed": 3}})
+    dr = DifferentiableRender(scene, r, 8 * 8)
+    alb = torch.from_numpy(triangle_albedo(prims)).to(cuda)
+    em = torch.from_numpy(light_emission(prims)).to(cuda)
+    with pytest.raises(native.LmgpuError) as e:
+        dr.forward(alb, em)
+    assert e.value.code == native.ERR_QUEUE_OVERFLOW
+    with pytest.raises(native.LmgpuError) as e:
+        dr.backward(alb, em, torch.ones((8, 8, 3), device=cuda))
+    assert e.value.code == native.ERR_QUEUE_OVERFLOW
+    r.configure({"rr_depth": -1, "max_path_vertices": 64, "sampler": {"rng_seed": 3}})
+    img = DifferentiableRender(scene, r, 8 * 8 * 4).forward(alb, em)
+    assert torch.isfinite(img).all() and float(img.max()) > 0
+    scene.close()

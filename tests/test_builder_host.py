@@ -65,3 +65,34 @@ def test_face_index_out_of_range_is_invalid():
     with pytest.raises(native.LmgpuError) as e:
         host_build(pos, faces)
     assert e.value.code == native.ERR_INVALID
+
+
+@pytest.mark.parametrize("ntris,sigma,seed", [(20000, 0.01, 1), (5000, 0.2, 5), (1, 0.1, 3), (2, 0.1, 4)])
+def test_render_tree_shape(ntris, sigma, seed):
+    """The render tree (binned SAH over three axes, leaves of at most 8
+    triangles) is a full binary tree over every triangle; the reference tree
+    of the same build is unchanged by it."""
+    pos, faces = random_soup(ntris, seed=seed, sigma=sigma)
+    info, order = host_build(pos, faces)
+    assert info.render_tree == native.RENDER_TREE_SAH
+    assert info.render_num_nodes == 2 * info.render_num_leaves - 1
+    assert info.render_num_leaves >= -(-ntris // 8)
+    assert info.render_max_depth <= max(1, ntris)
+    np.testing.assert_array_equal(order, oracle.OracleScene(pos, faces, "bvh").tri_order())
+
+
+def test_render_tree_degenerate_centroids_and_reference_option():
+    tri = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32)
+    pos = np.tile(tri, (300, 1))
+    faces = np.arange(900, dtype=np.uint32).reshape(-1, 3)
+    info, _ = host_build(pos, faces)
+    assert info.render_num_leaves == 1 and info.render_num_nodes == 1     # no axis can separate them
+    sc = Scene("bvh")
+    sc.load(soup_primitives(*random_soup(1000, seed=9, sigma=0.1)))
+    sc.configure({"render_tree": "reference"})
+    desc, keep = sc._describe()
+    inf = native.SceneInfo()
+    native.check(native.lib().lmgpu_scene_build_host(ctypes.byref(desc), ctypes.byref(inf), None, 0))
+    assert inf.render_tree == native.RENDER_TREE_REFERENCE and inf.render_num_nodes == inf.num_nodes
+    with pytest.raises(ValueError):
+        sc.configure({"render_tree": "quantised"})
