@@ -356,13 +356,16 @@ __global__ void __launch_bounds__(128) k_pt_init(const Ctx ctx, const PathState 
 
 // Closest-hit traversal of the queued rays (writes hit records). With a
 // scene table each ray is traced in its own path's scene.
-// Both path-tracer queues refill traversal lanes 24 at a time (measured on
-// the 1080p terrain: a few percent faster than 8).
+// Both path-tracer queues refill traversal lanes once 20 are idle and pause
+// a descent once fewer than 16 lanes still descend. Measured with the render
+// walks (1080p terrain frame / 64-scene batch): 166.7 / 793.9 ms against
+// 171.0 / 804.6 ms at (24, 24); pausing below 20 lanes or refilling 16 at a
+// time was slower, pausing below 28 slower still.
 #ifndef LMGPU_PT_REFILL_MIN
-#define LMGPU_PT_REFILL_MIN 24
+#define LMGPU_PT_REFILL_MIN 20
 #endif
 #ifndef LMGPU_PT_EXIT_BELOW
-#define LMGPU_PT_EXIT_BELOW 24
+#define LMGPU_PT_EXIT_BELOW 16
 #endif
 constexpr int PATH_QUEUE_REFILL_MIN = LMGPU_PT_REFILL_MIN;
 constexpr int PATH_QUEUE_EXIT_BELOW = LMGPU_PT_EXIT_BELOW;
