@@ -264,7 +264,7 @@ int create_impl(const LmgpuSceneDesc* desc, LmgpuScene** out)
     // (light.area.cpp:109-144).
     std::vector<AreaLightGpu> lights(desc->num_area_lights);
     std::vector<float> cdf;
-    std::vector<int32_t> ltris;
+    std::vector<int32_t> ltris, guide;
     for (int li = 0; li < desc->num_area_lights; li++) {
         AreaLightGpu& L = lights[li];
         std::memset(&L, 0, sizeof(L));
@@ -286,12 +286,22 @@ int create_impl(const LmgpuSceneDesc* desc, LmgpuScene** out)
         if (!(area > 0.0)) return fail(LMGPU_ERR_INVALID, "area light without area");
         for (double v : acc) cdf.push_back(float(v / area));
         L.num_tris = static_cast<int32_t>(acc.size() - 1);
+        // Guide of the CDF search: the same float comparison the device makes.
+        L.guide_begin = static_cast<int32_t>(guide.size());
+        const float* lc = cdf.data() + L.cdf_begin;
+        const int32_t n1 = L.num_tris + 1;
+        for (int j = 0; j <= LIGHT_GUIDE_BINS; j++) {
+            const float x = float(j) / float(LIGHT_GUIDE_BINS);
+            guide.push_back(static_cast<int32_t>(std::upper_bound(lc, lc + n1, x) - lc));
+        }
+        guide.push_back(n1);
         L.area = float(area);
         L.inv_area = float(1.0 / area);
     }
     up(lights, &d.area_lights);
     up(cdf, &d.light_cdf);
     up(ltris, &d.light_tris);
+    up(guide, &d.light_guide);
     d.num_area_lights = desc->num_area_lights;
     d.has_env = desc->has_env_light ? 1 : 0;
     d.num_lights = d.num_area_lights + d.has_env;

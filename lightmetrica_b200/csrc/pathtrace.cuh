@@ -127,8 +127,11 @@ __device__ __forceinline__ bool sample_light(const DeviceScene& s, float u0, flo
     }
     const AreaLightGpu L = s.area_lights[li];
     const float* cdf = s.light_cdf + L.cdf_begin;
-    // index = clamp(upper_bound(cdf, u1) - 1, 0, n - 1)
-    int lo = 0, hi = L.num_tris + 1;   // first element > u1 in [lo, hi)
+    // index = clamp(upper_bound(cdf, u1) - 1, 0, n - 1); the guide narrows
+    // the search to the entries between two of its starting points.
+    const int32_t* guide = s.light_guide + L.guide_begin;
+    const int gj = min(static_cast<int>(u1 * float(LIGHT_GUIDE_BINS)), LIGHT_GUIDE_BINS);
+    int lo = guide[gj], hi = guide[gj + 1];   // first element > u1 in [lo, hi), else hi
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
         if (cdf[mid] > u1) hi = mid; else lo = mid + 1;

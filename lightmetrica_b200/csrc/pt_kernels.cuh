@@ -369,6 +369,13 @@ __global__ void __launch_bounds__(128) k_pt_init(const Ctx ctx, const PathState 
 #endif
 constexpr int PATH_QUEUE_REFILL_MIN = LMGPU_PT_REFILL_MIN;
 constexpr int PATH_QUEUE_EXIT_BELOW = LMGPU_PT_EXIT_BELOW;
+// The shadow queue's any-hit walk may set its own.
+#ifndef LMGPU_PT_SHADOW_REFILL_MIN
+#define LMGPU_PT_SHADOW_REFILL_MIN LMGPU_PT_REFILL_MIN
+#endif
+#ifndef LMGPU_PT_SHADOW_EXIT_BELOW
+#define LMGPU_PT_SHADOW_EXIT_BELOW LMGPU_PT_EXIT_BELOW
+#endif
 
 template <bool TABLE>
 struct PathRayIO {
@@ -405,8 +412,8 @@ template <class Ctx>
 struct ShadowIO {
     static constexpr bool PER_RAY_SCENE = Ctx::TABLE;
     static constexpr bool RENDER = true;
-    static constexpr int REFILL_MIN = PATH_QUEUE_REFILL_MIN;
-    static constexpr int EXIT_BELOW = PATH_QUEUE_EXIT_BELOW;
+    static constexpr int REFILL_MIN = LMGPU_PT_SHADOW_REFILL_MIN;
+    static constexpr int EXIT_BELOW = LMGPU_PT_SHADOW_EXIT_BELOW;
     const uint32_t* count_ptr;
     const float4* sh_o;
     const float4* sh_d;

@@ -11,8 +11,15 @@ struct AreaLightGpu {
     float area, inv_area;
     int32_t cdf_begin;     // into DeviceScene::light_cdf / light_tris
     int32_t num_tris;
-    int32_t pad;
+    int32_t guide_begin;   // into DeviceScene::light_guide (LIGHT_GUIDE_BINS + 2 entries)
 };
+
+// Guide of a light's CDF search: guide[j] = the first CDF index whose value
+// exceeds j / LIGHT_GUIDE_BINS (j = 0 .. LIGHT_GUIDE_BINS), guide[BINS + 1] =
+// num_tris + 1. The index sought for u lies in [guide[j], guide[j + 1]] for
+// j = floor(u * BINS), so the search runs over a few entries and finds the
+// same index as a search over the whole CDF.
+constexpr int LIGHT_GUIDE_BINS = 256;
 
 // Pinhole camera (reference perspectivecamera.cpp:97-353). Matrices are
 // column-major 4x4 like Math::Mat4.
@@ -59,6 +66,7 @@ struct DeviceScene {
     const AreaLightGpu* area_lights;
     const float* light_cdf;       // per light: num_tris + 1 entries
     const int32_t* light_tris;    // triangle ids per light
+    const int32_t* light_guide;   // per light: LIGHT_GUIDE_BINS + 2 starting points of the CDF search
     float env_Le[3];
     float env_center[3];
     float env_radius;
