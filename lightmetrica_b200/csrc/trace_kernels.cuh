@@ -83,11 +83,12 @@ struct LaneScene {
 };
 
 
-template <int LAYOUT, int EXIT, bool RENDER, class Stack>
+template <int LAYOUT, int EXIT, bool RENDER, bool SPEC, class Stack>
 __device__ __forceinline__ bool descend(const LaneScene& s, TravState& ts, Stack stack, int cap,
-                                        const TraversalRay& r, bool may_exit, TraceStats* st)
+                                        const TraversalRay& r, bool may_exit, TraceStats* st, int32_t* pend)
 {
-    if (LAYOUT == LMGPU_LAYOUT_BVH2) return bvh2_descend<EXIT, RENDER>(s.bvh2, ts, stack, cap, r, st, may_exit);
+    if (LAYOUT == LMGPU_LAYOUT_BVH2)
+        return bvh2_descend<EXIT, RENDER, SPEC>(s.bvh2, ts, stack, cap, r, st, may_exit, pend);
     return bvh4_descend<EXIT, RENDER>(s.bvh4, ts, stack, cap, r, st, may_exit);
 }
 
@@ -122,6 +123,10 @@ __device__ __forceinline__ void add_trace_stats(const TraceStats& st, unsigned l
 // Shadow rays through binary nodes take the any-hit walk (bvh2_descend_any:
 // a stack of node references, no pop-time tests), whose visibility verdicts
 // equal the closest-hit walk's.
+// Render shadow rays through binary nodes descend speculatively (SPEC in
+// bvh2_descend_any; closest-hit render rays too with
+// LMGPU_TRACE_SPECULATIVE=2): each round a lane tests at most one leaf, the
+// one it postponed, and the warp's leaf tests fall in the same round.
 template <int LAYOUT, bool ANY_HIT>
 struct RefStackWalk : std::bool_constant<LMGPU_TRACE_ANYHIT_WALK && ANY_HIT && LAYOUT == LMGPU_LAYOUT_BVH2> {};
 
@@ -133,6 +138,8 @@ k_trace_persistent(const DeviceScene s, const IO io, int32_t* status, unsigned l
     constexpr unsigned FULL = 0xffffffffu;
     constexpr bool REFS = RefStackWalk<LAYOUT, ANY_HIT>::value;
     constexpr bool RENDER = render_rays<IO>::value;
+    constexpr bool SPEC = RENDER && LAYOUT == LMGPU_LAYOUT_BVH2 &&
+                          (REFS ? LMGPU_TRACE_SPECULATIVE >= 1 : LMGPU_TRACE_SPECULATIVE >= 2);
 #if LMGPU_TRACE_SHARED_STACK > 0
     // The shared part takes the same bytes either way: twice as many
     // 4-byte references as (reference, entry distance) pairs.
@@ -159,10 +166,11 @@ k_trace_persistent(const DeviceScene s, const IO io, int32_t* status, unsigned l
     TravState ts;
     ts.ref = REF_DONE;
     ts.sp = 0;
+    int32_t pend = 0;                          // postponed leaf (SPEC), 0: none
     int64_t idx = -1;
     bool exhausted = n <= 0;
     for (;;) {
-        const bool idle = ts.ref == REF_DONE;
+        const bool idle = ts.ref == REF_DONE && pend == 0;
         const unsigned need = __ballot_sync(FULL, idle);
         if (!exhausted && (__popc(need) >= refill_min<IO>::value || need == FULL)) {
             const int leader = __ffs(need) - 1;
@@ -191,14 +199,29 @@ k_trace_persistent(const DeviceScene s, const IO io, int32_t* status, unsigned l
         } else if (exhausted && need == FULL) {
             break;
         }
-        if (ts.ref != REF_DONE) {
-            bool ok;
-            if constexpr (REFS) ok = bvh2_descend_any<exit_below<IO>::value, RENDER>(ls.bvh2, ts, stack, cap, r, st, !exhausted);
-            else ok = descend<LAYOUT, exit_below<IO>::value, RENDER>(ls, ts, stack, cap, r, !exhausted, st);
+        if (ts.ref != REF_DONE || pend != 0) {
+            bool ok = true;
+            if (ts.ref != REF_DONE) {
+                if constexpr (REFS)
+                    ok = bvh2_descend_any<exit_below<IO>::value, RENDER, SPEC>(ls.bvh2, ts, stack, cap, r, st,
+                                                                             !exhausted, &pend);
+                else
+                    ok = descend<LAYOUT, exit_below<IO>::value, RENDER, SPEC>(ls, ts, stack, cap, r, !exhausted, st,
+                                                                            &pend);
+            }
             if (!ok) {
                 atomicOr(status, STATUS_STACK_OVERFLOW);
                 h.tri = -1;
                 ts.ref = REF_DONE;
+                pend = 0;
+            } else if (SPEC) {
+                // the postponed leaf; a leaf the descent stopped at is
+                // postponed by the next round's descent
+                if (pend != 0) {
+                    const int32_t leaf = pend;
+                    pend = 0;
+                    if (trace_leaf<ANY_HIT, RENDER>(ls.tris, ~leaf, r, h, st) && ANY_HIT) ts.ref = REF_DONE;
+                }
             } else if (ts.ref < 0) {           // at a leaf (a paused descent resumes next round)
                 // (a binary pop is the reference's far-child test; 4-wide
                 // nodes count their four slab tests when fetched)
