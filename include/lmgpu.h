@@ -39,7 +39,9 @@ enum {
     LMGPU_ERR_STACK_OVERFLOW = -4, /* traversal stack exceeded (device flag) */
     LMGPU_ERR_QUEUE_OVERFLOW = -5, /* wavefront queue exceeded (device flag) */
     LMGPU_ERR_TIMEOUT = -6,        /* a bounded device wait gave up */
-    LMGPU_ERR_UNSUPPORTED = -7     /* feature not available for this scene */
+    LMGPU_ERR_UNSUPPORTED = -7,    /* feature not available for this scene */
+    LMGPU_ERR_BOUNDS = -8          /* the bounds-checked build (liblmgpu_check.so) found
+                                      an index out of range (device flag) */
 };
 
 /* ------------------------------------------------------------- scene ---- */
@@ -360,7 +362,10 @@ int lmgpu_batch_set_config(LmgpuBatch* batch, const LmgpuBatchConfig* config);
  * or double by film_fp64; the caller zeroes it). All params share one
  * technique and one film type; wave_paths is ignored (the batch's
  * configuration sets it). Asynchronous on `stream` unless `stats` is given,
- * in which case the call synchronises and fills the totals of the batch. */
+ * in which case the call synchronises, fills the totals of the batch and
+ * reports the batch's device status (LMGPU_ERR_STACK_OVERFLOW,
+ * LMGPU_ERR_QUEUE_OVERFLOW); without `stats`, a status raised by the call
+ * is reported by the next call on the batch that synchronises. */
 int lmgpu_batch_render_device(LmgpuBatch* batch, const LmgpuRenderParams* params,
                               void* const* films_device, void* stream, LmgpuRenderStats* stats);
 

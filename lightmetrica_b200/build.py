@@ -54,48 +54,64 @@ def _stale(obj, deps):
     return any(os.path.exists(d) and os.path.getmtime(d) > t for d in deps)
 
 
+# Libraries built from the same sources: the product and the bounds-checked
+# build (tree references checked at scene build, every wavefront queue
+# append checked against its capacity; see LMGPU_BOUNDS_CHECK in
+# csrc/scene.cuh). The host builder object is shared.
+VARIANTS = [(OUT, BUILD_DIR, []),
+            (os.path.join(OUT_DIR, "liblmgpu_check.so"), os.path.join(BUILD_DIR, "check"), ["-DLMGPU_BOUNDS_CHECK=1"])]
+CHECK_OUT = VARIANTS[1][0]
+
+
 def build(verbose: bool = False, ptxas_verbose: bool = False) -> str:
+    """Compiles what is stale and links both libraries; returns the product's path."""
     os.makedirs(OUT_DIR, exist_ok=True)
-    os.makedirs(BUILD_DIR, exist_ok=True)
     # This file's flags are a dependency of every object too.
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(os.path.dirname(HERE), "include", "lmgpu.h"),
                                                        os.path.abspath(__file__)]
-    objs = []
     procs = []
-    for src in CU_SOURCES:
-        s = os.path.join(CSRC, src)
-        if not os.path.exists(s):
-            continue
-        o = os.path.join(BUILD_DIR, src + ".o")
-        objs.append(o)
-        if _stale(o, [s] + hdrs):
-            cmd = [_nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
-                   "-Xcompiler", "-ffp-contract=off", "--fmad=false", "-prec-div=false", "-prec-sqrt=false",
-                   "--expt-relaxed-constexpr",
-                   "-ccbin", _cxx(), "-c", s, "-o", o]
-            if ptxas_verbose:
-                cmd.insert(1, "-Xptxas=-v")
-            procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
+    host_objs = []
     for src in CPP_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD_DIR, src + ".o")
-        objs.append(o)
+        os.makedirs(BUILD_DIR, exist_ok=True)
+        host_objs.append(o)
         if _stale(o, [s] + hdrs):
             cmd = [_cxx(), "-O2", "-std=c++17", "-fPIC", "-pthread", "-ffp-contract=off", "-fno-fast-math",
                    "-c", s, "-o", o]
             procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
+    links = []
+    for out, bdir, defs in VARIANTS:
+        os.makedirs(bdir, exist_ok=True)
+        objs = []
+        for src in CU_SOURCES:
+            s = os.path.join(CSRC, src)
+            if not os.path.exists(s):
+                continue
+            o = os.path.join(bdir, src + ".o")
+            objs.append(o)
+            if _stale(o, [s] + hdrs):
+                cmd = [_nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
+                       "-Xcompiler", "-ffp-contract=off", "--fmad=false", "-prec-div=false", "-prec-sqrt=false",
+                       "--expt-relaxed-constexpr", *defs,
+                       "-ccbin", _cxx(), "-c", s, "-o", o]
+                if ptxas_verbose and not defs:
+                    cmd.insert(1, "-Xptxas=-v")
+                procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
+        links.append((out, objs + host_objs))
     for cmd, p in procs:
         out, _ = p.communicate()
         if verbose or ptxas_verbose or p.returncode != 0:
             sys.stdout.write(out)
         if p.returncode != 0:
             raise RuntimeError("compile failed: " + " ".join(cmd))
-    if _stale(OUT, objs):
-        cmd = [_nvcc(), *ARCH, "-shared", "-ccbin", _cxx(), "-o", OUT, *objs, "-Xcompiler", "-pthread"]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            sys.stdout.write(r.stdout + r.stderr)
-            raise RuntimeError("link failed")
+    for out, objs in links:
+        if _stale(out, objs):
+            cmd = [_nvcc(), *ARCH, "-shared", "-ccbin", _cxx(), "-o", out, *objs, "-Xcompiler", "-pthread"]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                sys.stdout.write(r.stdout + r.stderr)
+                raise RuntimeError("link failed: " + out)
     return OUT
 
 

@@ -2,6 +2,8 @@
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -37,6 +39,24 @@ int cuda_fail(cudaError_t e, const char* what)
     return LMGPU_ERR_CUDA;
 }
 
+int64_t check_limit_from_env(const char* name)
+{
+    const char* v = std::getenv(name);
+    if (!v || !*v) return INT64_MAX;
+    char* end = nullptr;
+    const long long x = std::strtoll(v, &end, 10);
+    return (end && *end == 0 && x >= 0) ? (int64_t)x : INT64_MAX;
+}
+
+int status_error(int32_t st)
+{
+    if (st & STATUS_BOUNDS) return fail(LMGPU_ERR_BOUNDS, "bounds check: index out of range");
+    if (st & STATUS_STACK_OVERFLOW) return fail(LMGPU_ERR_STACK_OVERFLOW, "traversal stack bound exceeded");
+    if (st & STATUS_QUEUE_OVERFLOW) return fail(LMGPU_ERR_QUEUE_OVERFLOW, "wavefront queue bound exceeded");
+    if (st & STATUS_TIMEOUT) return fail(LMGPU_ERR_TIMEOUT, "bounded device wait gave up");
+    return fail(LMGPU_ERR_CUDA, "unknown device status");
+}
+
 int consume_status(LmgpuScene* s, cudaStream_t stream)
 {
     int32_t st = 0;
@@ -44,10 +64,7 @@ int consume_status(LmgpuScene* s, cudaStream_t stream)
     LMGPU_CUDA_TRY(cudaStreamSynchronize(stream));
     if (st == 0) return LMGPU_OK;
     LMGPU_CUDA_TRY(cudaMemsetAsync(s->d_status, 0, sizeof(int32_t), stream));
-    if (st & STATUS_STACK_OVERFLOW) return fail(LMGPU_ERR_STACK_OVERFLOW, "traversal stack bound exceeded");
-    if (st & STATUS_QUEUE_OVERFLOW) return fail(LMGPU_ERR_QUEUE_OVERFLOW, "wavefront queue bound exceeded");
-    if (st & STATUS_TIMEOUT) return fail(LMGPU_ERR_TIMEOUT, "bounded device wait gave up");
-    return fail(LMGPU_ERR_CUDA, "unknown device status");
+    return status_error(st);
 }
 
 int resident_blocks_of(const void* kernel)
@@ -81,6 +98,63 @@ int upload(LmgpuScene* s, const std::vector<T>& v, const T** out)
     *out = static_cast<const T*>(p);
     return LMGPU_OK;
 }
+
+#if LMGPU_BOUNDS_CHECK
+// ---- tree references, checked on the device (bounds-checked build)
+// A walk follows only the references stored in the nodes, from the root: if
+// every internal reference is below the node limit and every leaf's run of
+// TriRecords ends (TRI_LAST_IN_LEAF) inside the triangle array, no walk
+// leaves the arrays. Leaves hold at most 255 triangles; a longer run fails.
+__device__ bool leaf_in_range(int32_t ref, const TriRecord* tris, int64_t ntris)
+{
+    const int64_t first = ~(int64_t)ref;
+    const int64_t end = first + 256 < ntris ? first + 256 : ntris;
+    for (int64_t k = first; k < end; k++)
+        if (tris[k].k_flags & TRI_LAST_IN_LEAF) return true;
+    return false;
+}
+__device__ bool ref_in_range(int32_t ref, int64_t limit, const TriRecord* tris, int64_t ntris)
+{
+    return ref >= 0 ? ref < limit : leaf_in_range(ref, tris, ntris);
+}
+// One thread per node; node n (n < num, the array's size) is read only.
+__global__ void k_check_bvh2(const Bvh2Node* nodes, int64_t num, int64_t limit, int32_t root,
+                             const TriRecord* tris, int64_t ntris, int32_t* status)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0 && !ref_in_range(root, limit, tris, ntris)) atomicOr(status, STATUS_BOUNDS);
+    if (i >= num) return;
+    if (!ref_in_range(nodes[i].left, limit, tris, ntris) || !ref_in_range(nodes[i].right, limit, tris, ntris))
+        atomicOr(status, STATUS_BOUNDS);
+}
+__global__ void k_check_bvh4(const Bvh4Node* nodes, int64_t num, int64_t limit, int32_t root,
+                             const TriRecord* tris, int64_t ntris, int32_t* status)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0 && !ref_in_range(root, limit, tris, ntris)) atomicOr(status, STATUS_BOUNDS);
+    if (i >= num) return;
+    for (int c = 0; c < 4; c++) {
+        const int32_t r = nodes[i].child[c];
+        if (r != BVH4_EMPTY && !ref_in_range(r, limit, tris, ntris)) atomicOr(status, STATUS_BOUNDS);
+    }
+}
+
+// Checks the uploaded trees of `d` (node counts n2 / n4, triangle count
+// ntris) into the scene's status word and consumes it.
+int check_trees(LmgpuScene* s, const DeviceScene& d, int64_t n2, int64_t n4, int64_t ntris)
+{
+    if (ntris <= 0) return LMGPU_OK;
+    const int64_t lim = check_limit_from_env("LMGPU_CHECK_NODE_LIMIT");
+    if (n2 > 0)
+        k_check_bvh2<<<(unsigned)((n2 + 127) / 128), 128>>>(d.bvh2, n2, std::min(n2, lim), d.root_ref, d.tris, ntris,
+                                                            s->d_status);
+    if (n4 > 0)
+        k_check_bvh4<<<(unsigned)((n4 + 127) / 128), 128>>>(d.bvh4, n4, std::min(n4, lim), d.root_ref4, d.tris, ntris,
+                                                            s->d_status);
+    LMGPU_CUDA_TRY(cudaGetLastError());
+    return consume_status(s, nullptr);
+}
+#endif
 
 // ---- camera matrices (reference math.transform.inl:88-113, perspectivecamera.cpp:97-160)
 bool mat_inverse(const double* m, double* inv)
@@ -345,6 +419,14 @@ int create_impl(const LmgpuSceneDesc* desc, LmgpuScene** out)
     s->d_status = static_cast<int32_t*>(st);
     s->d_work = reinterpret_cast<unsigned long long*>(static_cast<char*>(st) + 256);
     LMGPU_CUDA_TRY(cudaMemset(st, 0, scratch));
+#if LMGPU_BOUNDS_CHECK
+    if (desc->layout != LMGPU_LAYOUT_NAIVE) {
+        rc = check_trees(s, s->dev, (int64_t)b.bvh2.size(), (int64_t)b.bvh4.size(), (int64_t)b.tris.size());
+        if (rc == LMGPU_OK && render_tree)
+            rc = check_trees(s, s->rdev, (int64_t)b.rbvh2.size(), (int64_t)b.rbvh4.size(), (int64_t)b.rtris.size());
+        if (rc != LMGPU_OK) { lmgpu_scene_destroy(s); return rc; }
+    }
+#endif
 
     LmgpuSceneInfo& info = s->info;
     info.num_triangles = b.num_tris;

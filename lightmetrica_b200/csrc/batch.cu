@@ -430,6 +430,14 @@ int ensure_batch_workspace(LmgpuBatch* b, int64_t paths, int pools)
         st.depth = reinterpret_cast<int32_t*>(take(4 * P));
         st.free_slots = reinterpret_cast<int32_t*>(take(4 * P));
         st.retire = reinterpret_cast<int32_t*>(take(4 * P));
+        const uint32_t caps[4] = { (uint32_t)P, (uint32_t)P, (uint32_t)(2 * P), (uint32_t)P };
+        for (int q = 0; q < 4; q++) {
+            st.cap[q] = caps[q];
+#if LMGPU_BOUNDS_CHECK
+            st.cap[q] = (uint32_t)std::min<int64_t>(caps[q], check_limit_from_env("LMGPU_CHECK_QUEUE_LIMIT"));
+#endif
+        }
+        st.status = b->d_status;
     }
     b->ws_capacity = paths;
     b->ws_pools = pools;
@@ -458,8 +466,7 @@ int consume_batch_status(LmgpuBatch* b, cudaStream_t s)
     LMGPU_CUDA_TRY(cudaStreamSynchronize(s));
     if (v == 0) return LMGPU_OK;
     LMGPU_CUDA_TRY(cudaMemsetAsync(b->d_status, 0, sizeof(int32_t), s));
-    if (v & STATUS_STACK_OVERFLOW) return fail(LMGPU_ERR_STACK_OVERFLOW, "traversal stack bound exceeded");
-    return fail(LMGPU_ERR_CUDA, "unknown device status");
+    return status_error(v);
 }
 
 // Everything a render needs to know about its parameters.

@@ -54,6 +54,15 @@ int cuda_fail(cudaError_t e, const char* what);
 constexpr int32_t STATUS_STACK_OVERFLOW = 1;
 constexpr int32_t STATUS_QUEUE_OVERFLOW = 2;
 constexpr int32_t STATUS_TIMEOUT = 4;
+constexpr int32_t STATUS_BOUNDS = 8;       // bounds-checked build: an index out of range
+
+// The bounds-checked build (LMGPU_BOUNDS_CHECK=1, liblmgpu_check.so) takes
+// the limits its checks compare with from these variables when they are
+// set and lower than the real sizes (LMGPU_CHECK_NODE_LIMIT: tree nodes;
+// LMGPU_CHECK_QUEUE_LIMIT: wavefront queue slots), so that a test can make
+// a check fire while every access stays inside the buffers. Unset: no
+// limit (INT64_MAX). The unchecked build never reads them.
+int64_t check_limit_from_env(const char* name);
 
 // Path-tracer waves over caller-owned workspace memory (pathtrace.cu).
 int64_t workspace_paths_for_bytes(size_t bytes);
@@ -62,6 +71,8 @@ int render_device_preallocated(LmgpuScene* sc, const LmgpuRenderParams& p, void*
 
 // Reads and clears the device status word; maps it to an LMGPU status.
 int consume_status(LmgpuScene* s, cudaStream_t stream);
+// The LMGPU status (and message) of a non-zero device status word.
+int status_error(int32_t st);
 
 // The calling thread's current device must be the one the scene was created
 // on: the scene's buffers live there, and kernels launched elsewhere would

@@ -137,6 +137,7 @@ void carve_state(PathState& st, char* p, size_t P)
     st.sh_d = reinterpret_cast<float4*>(take(16 * P));
     st.sh_c = reinterpret_cast<float4*>(take(16 * P));
     st.raster = reinterpret_cast<float2*>(take(8 * P));
+    for (uint32_t& c : st.cap) c = (uint32_t)P;
 }
 
 int ensure_workspace(Workspace& ws, int64_t paths)
@@ -182,7 +183,12 @@ int render_waves(LmgpuScene* sc, const LmgpuRenderParams& p, F* film, cudaStream
         rc = ensure_workspace(ws, P);
     }
     if (rc != LMGPU_OK) return rc;
-    const PathState& st = ws.st;
+    PathState st = ws.st;
+    st.status = sc->d_status;
+#if LMGPU_BOUNDS_CHECK
+    const int64_t qlim = check_limit_from_env("LMGPU_CHECK_QUEUE_LIMIT");
+    for (uint32_t& q : st.cap) q = (uint32_t)std::min<int64_t>(q, qlim);
+#endif
     RenderConsts c;
     c.technique = TECH;
     c.rr_depth = p.rr_depth;
@@ -344,8 +350,6 @@ int ensure_host_film(HostFilmBuffers& hb, size_t film_bytes, size_t out_bytes)
     }
     return LMGPU_OK;
 }
-
-// Bytes of wave workspace per path (ensure_workspace's layout) and the
 
 // Points a Workspace at caller-owned memory (same layout as
 // ensure_workspace, no allocation); host_counts is the caller's readback

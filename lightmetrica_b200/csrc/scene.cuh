@@ -4,6 +4,15 @@
 #include <cstdint>
 #include "layout.h"
 
+// 1 in the bounds-checked build (liblmgpu_check.so): the scene build checks
+// every tree reference on the device, and every wavefront queue append is
+// checked against the queue's capacity; a failed check sets a status word
+// (LMGPU_ERR_BOUNDS / LMGPU_ERR_QUEUE_OVERFLOW), skips the access and never
+// traps. The traversal stack bound is checked in every build.
+#ifndef LMGPU_BOUNDS_CHECK
+#define LMGPU_BOUNDS_CHECK 0
+#endif
+
 namespace lmgpu {
 
 struct AreaLightGpu {

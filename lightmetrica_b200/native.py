@@ -11,8 +11,10 @@ import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 # The in-tree build; LMGPU_LIBRARY names another build of the same sources
-# (for example one compiled with different tuning constants).
+# (the bounds-checked CHECK_LIB_PATH, or one compiled with different tuning
+# constants).
 LIB_PATH = os.environ.get("LMGPU_LIBRARY") or os.path.join(HERE, "_lib", "liblmgpu.so")
+CHECK_LIB_PATH = os.path.join(HERE, "_lib", "liblmgpu_check.so")
 
 c_int32 = ctypes.c_int32
 c_int64 = ctypes.c_int64
@@ -31,9 +33,10 @@ ERR_STACK_OVERFLOW = -4
 ERR_QUEUE_OVERFLOW = -5
 ERR_TIMEOUT = -6
 ERR_UNSUPPORTED = -7
+ERR_BOUNDS = -8
 STATUS_NAMES = {OK: "OK", ERR_INVALID: "INVALID", ERR_OOM: "OOM", ERR_CUDA: "CUDA",
                 ERR_STACK_OVERFLOW: "STACK_OVERFLOW", ERR_QUEUE_OVERFLOW: "QUEUE_OVERFLOW",
-                ERR_TIMEOUT: "TIMEOUT", ERR_UNSUPPORTED: "UNSUPPORTED"}
+                ERR_TIMEOUT: "TIMEOUT", ERR_UNSUPPORTED: "UNSUPPORTED", ERR_BOUNDS: "BOUNDS"}
 
 LAYOUT_BVH2, LAYOUT_BVH4, LAYOUT_NAIVE = 0, 1, 2
 RENDER_TREE_SAH, RENDER_TREE_REFERENCE = 0, 1

@@ -4,6 +4,8 @@ import ctypes
 import os
 import re
 
+import pytest
+
 from lightmetrica_b200 import native
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -21,8 +23,9 @@ def test_header_declares_entry_points():
         assert s in syms
 
 
-def test_library_exports_every_declared_symbol():
-    lib = ctypes.CDLL(native.LIB_PATH)
+@pytest.mark.parametrize("path", [native.LIB_PATH, native.CHECK_LIB_PATH], ids=["product", "bounds_checked"])
+def test_library_exports_every_declared_symbol(path):
+    lib = ctypes.CDLL(path)
     missing = [s for s in declared_symbols() if not hasattr(lib, s)]
     assert not missing, f"missing exports: {missing}"
 
