@@ -54,6 +54,7 @@ struct DiffConsts {
     int32_t technique, rr_depth, max_pv, sampling;
     uint64_t seed;
     int64_t sample_offset, num_samples, pixels;
+    double inv_pixels;       // 1 / pixels
     float scale;             // film rescale W*H/num_samples
     const float* albedo;     // 3 per triangle or null
     const float* emission;   // 3 per area light or null
@@ -366,9 +367,7 @@ __global__ void __launch_bounds__(128, 8) k_diff(const DeviceScene s, const Diff
         const float u0 = rng_uniform(key, DIM_RASTER), u1 = rng_uniform(key, DIM_RASTER + 1);
         float rx, ry;
         if (c.sampling == LMGPU_SAMPLING_STRATIFIED) {
-            const int64_t pix = (int64_t)(sample % (uint64_t)c.pixels);
-            rx = (float(pix % s.cam.width) + u0) / float(s.cam.width);
-            ry = (float(pix / s.cam.width) + u1) / float(s.cam.height);
+            stratified_raster((int64_t)sample, c.pixels, c.inv_pixels, s.cam.width, s.cam.height, u0, u1, rx, ry);
         } else {
             rx = u0; ry = u1;
         }
@@ -473,6 +472,8 @@ int launch_diff(LmgpuScene* sc, const LmgpuRenderParams* p, const LmgpuDiffParam
     if (const int rc = check_scene_device(sc)) return rc;
     if (!sc->dev.cam.valid) return fail(LMGPU_ERR_INVALID, "scene has no camera");
     if (p->num_samples <= 0) return fail(LMGPU_ERR_INVALID, "num_samples must be positive");
+    if (p->sample_offset < 0) return fail(LMGPU_ERR_INVALID, "negative sample offset");
+    if (!sample_range_ok(p->sample_offset, p->num_samples)) return fail(LMGPU_ERR_INVALID, "sample indices reach 2^53");
     if (p->technique < LMGPU_RENDER_PT || p->technique > LMGPU_RENDER_PT_MIS) return fail(LMGPU_ERR_INVALID, "unknown technique");
     DiffConsts c;
     std::memset(&c, 0, sizeof(c));
@@ -484,6 +485,7 @@ int launch_diff(LmgpuScene* sc, const LmgpuRenderParams* p, const LmgpuDiffParam
     c.sample_offset = p->sample_offset;
     c.num_samples = p->num_samples;
     c.pixels = (int64_t)sc->dev.cam.width * sc->dev.cam.height;
+    c.inv_pixels = 1.0 / double(c.pixels);
     c.scale = float(double(c.pixels) / double(p->num_samples));
     c.albedo = dp ? dp->albedo : nullptr;
     c.emission = dp ? dp->emission : nullptr;

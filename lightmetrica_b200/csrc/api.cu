@@ -192,6 +192,7 @@ bool setup_camera(const LmgpuSceneDesc& d, CameraGpu& cam)
     std::memset(&cam, 0, sizeof(cam));
     if (!d.has_camera) return true;
     if (d.film_width <= 0 || d.film_height <= 0 || !(d.camera_fovy_degrees > 0.0f)) return false;
+    if ((int64_t)d.film_width * d.film_height >= (int64_t(1) << 31)) return false;   // pixel indices are 32-bit
     double eye[3], ctr[3], up[3];
     for (int i = 0; i < 3; i++) { eye[i] = d.camera_eye[i]; ctr[i] = d.camera_center[i]; up[i] = d.camera_up[i]; }
     // LookAt: f = normalize(center - eye), s = normalize(f x up), u = s x f

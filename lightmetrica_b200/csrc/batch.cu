@@ -495,6 +495,7 @@ int make_plan(LmgpuBatch* b, const LmgpuRenderParams* params, void* const* films
         if (p.sampling != LMGPU_SAMPLING_STRATIFIED && p.sampling != LMGPU_SAMPLING_UNIFORM) return fail(LMGPU_ERR_INVALID, "unknown sampling");
         if (p.num_samples <= 0) return fail(LMGPU_ERR_INVALID, "num_samples must be positive");
         if (p.sample_offset < 0) return fail(LMGPU_ERR_INVALID, "negative sample offset");
+        if (!sample_range_ok(p.sample_offset, p.num_samples)) return fail(LMGPU_ERR_INVALID, "sample indices reach 2^53");
         if (!sc->dev.cam.valid) return fail(LMGPU_ERR_INVALID, "scene has no camera");
         pl.total += p.num_samples;
         if (p.max_path_vertices == -1) pl.bounded = false;
@@ -532,6 +533,7 @@ int upload_table(LmgpuBatch* b, const LmgpuRenderParams* params, void* const* fi
         e.rc.seed = p.seed;
         e.rc.sample_base = p.sample_offset;
         e.rc.pixels = (int64_t)e.s.cam.width * e.s.cam.height;
+        e.rc.inv_pixels = 1.0 / double(e.rc.pixels);
         e.begin = begin;
         e.film = films[i];
         b->h_begins[i] = begin;

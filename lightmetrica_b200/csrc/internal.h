@@ -74,6 +74,14 @@ int consume_status(LmgpuScene* s, cudaStream_t stream);
 // The LMGPU status (and message) of a non-zero device status word.
 int status_error(int32_t st);
 
+// Sample indices of a render stay below 2^53 (stratified_raster's
+// double-precision quotient); offset and count are non-negative.
+inline bool sample_range_ok(int64_t offset, int64_t count)
+{
+    constexpr int64_t LIMIT = int64_t(1) << 53;
+    return offset < LIMIT && count <= LIMIT - offset;
+}
+
 // The calling thread's current device must be the one the scene was created
 // on: the scene's buffers live there, and kernels launched elsewhere would
 // read another GPU's memory.

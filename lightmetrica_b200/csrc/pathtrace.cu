@@ -196,6 +196,7 @@ int render_waves(LmgpuScene* sc, const LmgpuRenderParams& p, F* film, cudaStream
     c.sampling = p.sampling;
     c.seed = p.seed;
     c.pixels = pixels;
+    c.inv_pixels = 1.0 / double(pixels);
     const int shade_blocks = 148 * 8;
     for (int64_t base = 0; base < p.num_samples && rc == LMGPU_OK; base += P) {
         const int64_t cnt = std::min<int64_t>(P, p.num_samples - base);
@@ -263,6 +264,7 @@ int check_params(LmgpuScene* sc, const LmgpuRenderParams* p)
     if (!sc->dev.cam.valid) return fail(LMGPU_ERR_INVALID, "scene has no camera");
     if (p->num_samples <= 0) return fail(LMGPU_ERR_INVALID, "num_samples must be positive");
     if (p->sample_offset < 0) return fail(LMGPU_ERR_INVALID, "negative sample offset");
+    if (!sample_range_ok(p->sample_offset, p->num_samples)) return fail(LMGPU_ERR_INVALID, "sample indices reach 2^53");
     if (p->technique < LMGPU_RENDER_PT || p->technique > LMGPU_RENDER_PT_MIS) return fail(LMGPU_ERR_INVALID, "unknown technique");
     if (p->sampling != LMGPU_SAMPLING_STRATIFIED && p->sampling != LMGPU_SAMPLING_UNIFORM) return fail(LMGPU_ERR_INVALID, "unknown sampling");
     if (p->wave_paths < 0) return fail(LMGPU_ERR_INVALID, "negative wave size");
@@ -383,6 +385,7 @@ int render_device_preallocated(LmgpuScene* sc, const LmgpuRenderParams& p, void*
     if (!sc->dev.cam.valid) return fail(LMGPU_ERR_INVALID, "scene has no camera");
     if (p.num_samples <= 0) return fail(LMGPU_ERR_INVALID, "num_samples must be positive");
     if (p.sample_offset < 0) return fail(LMGPU_ERR_INVALID, "negative sample offset");
+    if (!sample_range_ok(p.sample_offset, p.num_samples)) return fail(LMGPU_ERR_INVALID, "sample indices reach 2^53");
     if (p.technique < LMGPU_RENDER_PT || p.technique > LMGPU_RENDER_PT_MIS) return fail(LMGPU_ERR_INVALID, "unknown technique");
     if (p.sampling != LMGPU_SAMPLING_STRATIFIED && p.sampling != LMGPU_SAMPLING_UNIFORM) return fail(LMGPU_ERR_INVALID, "unknown sampling");
     if (p.wave_paths < 0) return fail(LMGPU_ERR_INVALID, "negative wave size");

@@ -56,6 +56,25 @@ __device__ __forceinline__ float camera_importance(const CameraGpu& c, float cos
     return c.inv_A * inv * inv * inv;
 }
 
+// Raster position of a stratified sample: pixel = sample mod (W*H), then
+// ((x + u0) / W, (y + u1) / H). The render entry points keep the sample
+// index below 2^53 and W*H below 2^31, so the quotient is estimated in
+// double precision (the operands are exact and the product's relative
+// error is below 2^-52: the estimate is off by at most one, then corrected)
+// and the row and column come from a 32-bit division; the result equals
+// the 64-bit integer remainder's.
+__device__ __forceinline__ void stratified_raster(int64_t sample, int64_t pixels, double inv_pixels, int width,
+                                                  int height, float u0, float u1, float& rx, float& ry)
+{
+    const int64_t q = (int64_t)(double(sample) * inv_pixels);
+    int64_t pix = sample - q * pixels;
+    if (pix < 0) pix += pixels;
+    else if (pix >= pixels) pix -= pixels;
+    const uint32_t w = (uint32_t)width, y = (uint32_t)pix / w, x = (uint32_t)pix - y * w;
+    rx = (float(x) + u0) / float(width);
+    ry = (float(y) + u1) / float(height);
+}
+
 // SampleAndEstimateDirection (perspectivecamera.cpp:216-240): raster in
 // [0,1]^2 -> world direction; pdf = importance (projected solid angle);
 // the estimated weight We/pdf is 1.

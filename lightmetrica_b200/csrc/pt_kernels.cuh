@@ -75,6 +75,7 @@ struct RenderConsts {
     uint64_t seed;
     int64_t sample_base;   // OneScene: sample index of the wave's path 0; SceneTable: the scene's sample offset
     int64_t pixels;
+    double inv_pixels;     // 1 / pixels
 };
 
 // ------------------------------------------------------------ contexts ----
@@ -341,9 +342,7 @@ __global__ void __launch_bounds__(128) k_pt_init(const Ctx ctx, const PathState 
     const float u0 = rng_uniform(key, DIM_RASTER), u1 = rng_uniform(key, DIM_RASTER + 1);
     float rx, ry;
     if (rc.sampling == LMGPU_SAMPLING_STRATIFIED) {
-        const int64_t pix = (int64_t)((uint64_t)sample % (uint64_t)rc.pixels);
-        rx = (float(pix % s.cam.width) + u0) / float(s.cam.width);
-        ry = (float(pix / s.cam.width) + u1) / float(s.cam.height);
+        stratified_raster(sample, rc.pixels, rc.inv_pixels, s.cam.width, s.cam.height, u0, u1, rx, ry);
     } else {
         rx = u0; ry = u1;
     }
