@@ -399,7 +399,7 @@ int lmgpu_batch_profile(LmgpuBatch* batch, const LmgpuRenderParams* params, void
 
 /* Autotuner: renders the batch with each scene's sample count scaled by
  * `sample_fraction` (0 < f <= 1; raised for a candidate until the trial
- * holds four of its waves, or the whole render) under candidate
+ * holds four of its waves, eight in overlap mode, or the whole render) under candidate
  * configurations (mode, BVH layout, paths in flight, shading grid, overlap
  * bounce), coordinate by coordinate, keeps the one with the least device
  * time per sample, stores it as the batch's configuration and returns it

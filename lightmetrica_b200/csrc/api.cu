@@ -375,7 +375,21 @@ int create_impl(const LmgpuSceneDesc* desc, LmgpuScene** out)
     }
     up(lights, &d.area_lights);
     up(cdf, &d.light_cdf);
-    up(ltris, &d.light_tris);
+    std::vector<float4> lrecs;
+    lrecs.reserve(3 * ltris.size());
+    for (int li = 0; li < desc->num_area_lights; li++) {
+        const AreaLightGpu& L = lights[li];
+        for (int32_t k = 0; k < L.num_tris; k++) {
+            const int64_t t = ltris[(size_t)(L.cdf_begin - li + k)];
+            const float* p[3];
+            for (int c = 0; c < 3; c++) p[c] = &b.positions[3 * (size_t)b.tri_vidx[3 * t + c]];
+            const float c0 = cdf[(size_t)(L.cdf_begin + k)], c1 = cdf[(size_t)(L.cdf_begin + k + 1)];
+            lrecs.push_back(make_float4(p[0][0], p[0][1], p[0][2], p[1][0]));
+            lrecs.push_back(make_float4(p[1][1], p[1][2], p[2][0], p[2][1]));
+            lrecs.push_back(make_float4(p[2][2], c0, c1, 0.0f));
+        }
+    }
+    up(lrecs, &d.light_recs);
     up(guide, &d.light_guide);
     d.num_area_lights = desc->num_area_lights;
     d.has_env = desc->has_env_light ? 1 : 0;

@@ -1086,13 +1086,17 @@ int lmgpu_batch_autotune(LmgpuBatch* b, const LmgpuRenderParams* params, double 
     const LmgpuBatchConfig start = b->cfg;
     // A candidate is timed on at least four of its own waves (or the whole
     // render), so that large waves are not judged on a render that one wave
-    // holds, and is compared by device time per sample.
+    // holds, and is compared by device time per sample. Overlap mode gets
+    // four of its periods (eight waves): its first head and last tail run
+    // alone, and on a four-wave trial of the 64-scene batch that hid its
+    // gain (overlap 780 ms, fixed waves 816 ms on the whole batch).
     auto trial = [&](const LmgpuBatchConfig& c, double& ms_per_sample) -> int {
         int r = check_config(c);
         if (r != LMGPU_OK) return r;
         ms_per_sample = 1e30;
         b->cfg = c;
-        const double f = std::min(1.0, std::max(fraction, 4.0 * (double)c.wave_paths / (double)full));
+        const double waves_needed = c.mode == LMGPU_BATCH_OVERLAP ? 8.0 : 4.0;
+        const double f = std::min(1.0, std::max(fraction, waves_needed * (double)c.wave_paths / (double)full));
         const int64_t samples = scale(f);
         LmgpuRenderStats st;
         if ((r = batch_render(b, p.data(), films.data(), s, &st)) != LMGPU_OK) return r;   // warm-up (capture)

@@ -151,16 +151,26 @@ __device__ __forceinline__ bool sample_light(const DeviceScene& s, float u0, flo
     const int32_t* guide = s.light_guide + L.guide_begin;
     const int gj = min(static_cast<int>(u1 * float(LIGHT_GUIDE_BINS)), LIGHT_GUIDE_BINS);
     int lo = guide[gj], hi = guide[gj + 1];   // first element > u1 in [lo, hi), else hi
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (cdf[mid] > u1) hi = mid; else lo = mid + 1;
+    if (hi - lo <= LIGHT_SCAN) {
+        // The CDF does not decrease: the entries <= u1 are a prefix of the
+        // range, counted with independent loads instead of dependent halvings.
+        int below = 0;
+#pragma unroll
+        for (int k = 0; k < LIGHT_SCAN; k++)
+            if (lo + k < hi && cdf[lo + k] <= u1) below++;
+        lo += below;
+    } else {
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (cdf[mid] > u1) hi = mid; else lo = mid + 1;
+        }
     }
     const int idx = min(max(lo - 1, 0), L.num_tris - 1);
-    const float c0 = cdf[idx], c1 = cdf[idx + 1];
+    const float4* rec = s.light_recs + 3 * (L.cdf_begin - li + idx);
+    const float4 q0 = rec[0], q1 = rec[1], q2 = rec[2];
+    const float c0 = q2.y, c1 = q2.z;          // cdf[idx], cdf[idx + 1]
     const float v = (u1 - c0) / (c1 - c0);
-    const int tri = s.light_tris[L.cdf_begin - li + idx];   // light_tris is packed without the cdf's extra entry
-    const uint32_t i1 = s.tri_vidx[3 * tri], i2 = s.tri_vidx[3 * tri + 1], i3 = s.tri_vidx[3 * tri + 2];
-    const V3 p1 = load3(s.vpos + 3 * i1), p2 = load3(s.vpos + 3 * i2), p3 = load3(s.vpos + 3 * i3);
+    const V3 p1 = v3(q0.x, q0.y, q0.z), p2 = v3(q0.w, q1.x, q1.y), p3 = v3(q1.z, q1.w, q2.x);
     // UniformSampleTriangle (math.stats.inl:120-125)
     const float sq = sqrtf(fmaxf(0.0f, u0));
     const float b0 = 1.0f - sq, b1 = v * sq;

@@ -18,7 +18,7 @@ namespace lmgpu {
 struct AreaLightGpu {
     float Le[3];
     float area, inv_area;
-    int32_t cdf_begin;     // into DeviceScene::light_cdf / light_tris
+    int32_t cdf_begin;     // into DeviceScene::light_cdf; light_recs from cdf_begin - (light index)
     int32_t num_tris;
     int32_t guide_begin;   // into DeviceScene::light_guide (LIGHT_GUIDE_BINS + 2 entries)
 };
@@ -29,6 +29,9 @@ struct AreaLightGpu {
 // j = floor(u * BINS), so the search runs over a few entries and finds the
 // same index as a search over the whole CDF.
 constexpr int LIGHT_GUIDE_BINS = 256;
+// Guide ranges of at most this many CDF entries are scanned, longer ones
+// halved (sample_light).
+constexpr int LIGHT_SCAN = 8;
 
 // Pinhole camera (reference perspectivecamera.cpp:97-353). Matrices are
 // column-major 4x4 like Math::Mat4.
@@ -74,7 +77,12 @@ struct DeviceScene {
     int32_t has_env;
     const AreaLightGpu* area_lights;
     const float* light_cdf;       // per light: num_tris + 1 entries
-    const int32_t* light_tris;    // triangle ids per light
+    // Per light triangle, in CDF order (entry cdf_begin - li + idx for light
+    // li): its vertices p1, p2, p3 and the CDF values around it, cdf[idx]
+    // and cdf[idx + 1], as 3 float4 (p1.xyz p2.x | p2.yz p3.xy | p3.z c0 c1 -):
+    // one 48-byte record instead of the chain triangle id -> vertex indices
+    // -> positions after the CDF search.
+    const float4* light_recs;
     const int32_t* light_guide;   // per light: LIGHT_GUIDE_BINS + 2 starting points of the CDF search
     float env_Le[3];
     float env_center[3];
