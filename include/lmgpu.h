@@ -421,6 +421,9 @@ int lmgpu_batch_autotune(LmgpuBatch* batch, const LmgpuRenderParams* params, dou
  *                                (perspectivecamera.cpp:304-323)
  *   lmgpu_film_pixels            the pixel HDRBitmapFilm::AccumulateContribution
  *                                adds a raster position to (hdrfilm.cpp:151-171)
+ *   lmgpu_light_sample           Scene::SampleLightSelection (scene.cpp:79-86) and
+ *                                the light's SamplePosition (light.area.cpp:146-179,
+ *                                light.env.const.cpp:194-203)
  *   lmgpu_bsdf_sample            BSDF::SampleAndEstimateDirection, transport
  *                                EL (diffuse.cpp:133-157, mirror.cpp:84-107,
  *                                diffusemirror.cpp:84-125)
@@ -444,6 +447,10 @@ int lmgpu_camera_raster_positions(const LmgpuScene* scene, const float* rays, in
 /* Raster positions (n x 2) -> pixel index y * W + x of the scene camera's
  * film (n; -1 outside [0,1]^2), as the renderers' film splats map them. */
 int lmgpu_film_pixels(const LmgpuScene* scene, const float* raster, int64_t n, int32_t* pixel);
+/* The scene's lights: (u0, u1) (n x 2) -> a point on the light chosen by u0
+ * (n x 7: position, normal, area pdf times the selection probability) and
+ * its index (n; num_area_lights for the environment, -1 without lights). */
+int lmgpu_light_sample(const LmgpuScene* scene, const float* u, int64_t n, float* points, int32_t* light);
 
 /* BSDF `type` (LMGPU_BSDF_*) with reflectance R (3 floats) at frames given by
  * geometric and shading normals (n x 6: gn, sn; tangents from sn as

@@ -80,6 +80,18 @@ def film_pixels(scene, raster):
     return out
 
 
+def light_sample(scene, u):
+    """(u0, u1) (n x 2) -> dict of position, normal (n x 3), pdf (n: area pdf
+    times the light selection probability) and light (n: area light index,
+    the number of area lights for the environment), as the renderers' next
+    event estimation samples the scene's lights."""
+    uu = _f32(u, 2)
+    pts = np.empty((uu.shape[0], 7), dtype=np.float32)
+    light = np.empty(uu.shape[0], dtype=np.int32)
+    N.check(N.lib().lmgpu_light_sample(scene.handle, _p(uu), uu.shape[0], _p(pts), _p(light)))
+    return {"position": pts[:, 0:3], "normal": pts[:, 3:6], "pdf": pts[:, 6], "light": light}
+
+
 def bsdf_sample(bsdf, reflectance, frames, wi, u):
     """SampleAndEstimateDirection (EL) -> dict of wo, weight (n x 3), pdf (n,
     projected solid angle), specular (n)."""

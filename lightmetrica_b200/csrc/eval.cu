@@ -67,6 +67,27 @@ __global__ void k_camera_raster(const CameraGpu cam, const float* __restrict__ r
     }
 }
 
+// Scene::SampleLightSelection + the light's SamplePosition (sample_light)
+// for given (u0, u1): position, normal, area pdf with the selection
+// probability, and the light index per sample (-1 if the scene has no light).
+__global__ void k_light_sample(const DeviceScene s, const float* __restrict__ u, int64_t n, float* __restrict__ out,
+                               int32_t* __restrict__ light)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        LightPoint lp;
+        float* o = out + 7 * i;
+        if (sample_light(s, u[2 * i], u[2 * i + 1], lp)) {
+            o[0] = lp.p.x; o[1] = lp.p.y; o[2] = lp.p.z;
+            o[3] = lp.n.x; o[4] = lp.n.y; o[5] = lp.n.z;
+            o[6] = lp.pdf_area;
+            light[i] = lp.light;
+        } else {
+            for (int c = 0; c < 7; c++) o[c] = 0.0f;
+            light[i] = -1;
+        }
+    }
+}
+
 __global__ void k_film_pixels(const CameraGpu cam, const float* __restrict__ raster, int64_t n, int32_t* __restrict__ pixel)
 {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -232,6 +253,26 @@ int lmgpu_camera_raster_positions(const LmgpuScene* scene, const float* rays, in
     void* dst[2] = { raster, valid };
     void* src[2] = { d_out, d_valid };
     const size_t bytes[2] = { b_out, b_valid };
+    return finish(dst, src, bytes, 2);
+}
+
+int lmgpu_light_sample(const LmgpuScene* scene, const float* u, int64_t n, float* points, int32_t* light)
+{
+    if (!scene) return fail(LMGPU_ERR_INVALID, "null scene");
+    int rc = check_count(n);
+    if (rc != LMGPU_OK || n == 0) return rc;
+    if (!u || !points || !light) return fail(LMGPU_ERR_INVALID, "null argument");
+    const size_t b_u = (size_t)n * 2 * sizeof(float), b_p = (size_t)n * 7 * sizeof(float), b_l = (size_t)n * 4;
+    Scratch s;
+    if ((rc = s.reserve(padded(b_u) + padded(b_p) + padded(b_l))) != LMGPU_OK) return rc;
+    float* d_u = s.take<float>((size_t)n * 2);
+    float* d_p = s.take<float>((size_t)n * 7);
+    int32_t* d_l = s.take<int32_t>((size_t)n);
+    if ((rc = copy_in(d_u, u, b_u)) != LMGPU_OK) return rc;
+    k_light_sample<<<eval_blocks(n), 128>>>(scene->dev, d_u, n, d_p, d_l);
+    void* dst[2] = { points, light };
+    void* src[2] = { d_p, d_l };
+    const size_t bytes[2] = { b_p, b_l };
     return finish(dst, src, bytes, 2);
 }
 

@@ -119,6 +119,7 @@ struct LightPoint {
     V3 p, n;            // position and normal (gn = sn)
     float pdf_area;     // area pdf including the selection probability
     V3 Le;
+    int light;          // area light index, num_area_lights for the environment
 };
 
 // Scene::SampleLightSelection (scene.cpp:79-86, reuses u0) followed by
@@ -142,6 +143,7 @@ __device__ __forceinline__ bool sample_light(const DeviceScene& s, float u0, flo
         lp.n = -d;
         lp.pdf_area = s.env_inv_area * sel;
         lp.Le = load3(s.env_Le);
+        lp.light = li;
         return true;
     }
     const AreaLightGpu L = s.area_lights[li];
@@ -178,6 +180,7 @@ __device__ __forceinline__ bool sample_light(const DeviceScene& s, float u0, flo
     lp.n = normalize(cross(p2 - p1, p3 - p1));
     lp.pdf_area = L.inv_area * sel;
     lp.Le = load3(L.Le);
+    lp.light = li;
     return true;
 }
 

@@ -150,6 +150,7 @@ SIGNATURES = {
     "lmgpu_camera_sample_rays": (c_int32, [c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
     "lmgpu_camera_raster_positions": (c_int32, [c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
     "lmgpu_film_pixels": (c_int32, [c_void_p, c_void_p, c_int64, c_void_p]),
+    "lmgpu_light_sample": (c_int32, [c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
     "lmgpu_bsdf_sample": (c_int32, [c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p,
                                     c_void_p, c_void_p]),
     "lmgpu_bsdf_evaluate": (c_int32, [c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),

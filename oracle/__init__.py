@@ -613,6 +613,23 @@ def _camera_desc(eye, center, up, fovy, width, height):
     return d
 
 
+def light_sample(prims, u):
+    """The C restatement's light sample (scene.cpp:79-86, light.area.cpp:146-179,
+    light.env.const.cpp:194-203) of the scene's lights for (u0, u1) (n x 2):
+    (points (n x 7: position, normal, area pdf times the selection
+    probability), light index (n))."""
+    L = lib()
+    L.orc_light_sample.restype = ctypes.c_int
+    L.orc_light_sample.argtypes = [ctypes.POINTER(_OrcPtDesc), ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                   ctypes.c_void_p]
+    d, keep = _pt_desc(prims, "pt.mis", 1, -1, 1, "stratified", None, None)
+    uu = _f64(u, 2)
+    out, light = np.empty((uu.shape[0], 7)), np.empty(uu.shape[0], dtype=np.int32)
+    if not L.orc_light_sample(ctypes.byref(d), _ptr(uu), uu.shape[0], _ptr(out), _ptr(light)):
+        raise ValueError("scene setup failed")
+    return out, light
+
+
 def camera_rays(raster, eye, center, up, fovy, width, height):
     """Raster positions (n x 2) -> (origins and directions (n x 6), pdf (n))."""
     r = _f64(raster, 2)

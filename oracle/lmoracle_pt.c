@@ -819,6 +819,31 @@ int orc_camera_rays(const orc_pt_desc* d, const double* raster, int n, double* r
     return ok;
 }
 
+/* The lights of d: (u0, u1) (n x 2) -> the point sample_light draws
+ * (position, normal, area pdf times the selection probability; n x 7) and
+ * the light index (n; num_lights for the environment, -1 without lights).
+ * Returns 0 if the scene cannot be set up. */
+int orc_light_sample(const orc_pt_desc* d, const double* u, int n, double* out, int* light)
+{
+    pt_scene s;
+    const int ok = setup(&s, d);
+    for (int i = 0; ok && i < n; i++) {
+        lpoint lp;
+        double* o = out + 7 * i;
+        if (sample_light(&s, u[2 * i], u[2 * i + 1], &lp)) {
+            o[0] = lp.p.x; o[1] = lp.p.y; o[2] = lp.p.z;
+            o[3] = lp.n.x; o[4] = lp.n.y; o[5] = lp.n.z;
+            o[6] = lp.pdf;
+            light[i] = lp.light;
+        } else {
+            for (int c = 0; c < 7; c++) o[c] = 0.0;
+            light[i] = -1;
+        }
+    }
+    teardown(&s);
+    return ok;
+}
+
 /* RayToRasterPosition: rays (n x 6) -> raster (n x 2) and valid (n; 0 when
  * the direction leaves the film). Returns 0 for a degenerate camera. */
 int orc_camera_raster(const orc_pt_desc* d, const double* rays, int n, double* raster, int* valid)

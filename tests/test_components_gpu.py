@@ -176,3 +176,55 @@ def test_film_pixels_match_host_film(cuda):
     np.testing.assert_array_equal(got, want)
     assert got[0] == 0 and got[1] == W * H - 1
     s.close()
+
+
+def light_scene(level):
+    """Two area lights and the constant environment: an icosphere light of
+    `level` (level 1: 80 triangles, at most a few CDF entries per guide bin,
+    which the device scans; level 5: 20,480, about 80 per bin, which it
+    halves) and a two-triangle quad light of another area and luminance."""
+    from lightmetrica_b200 import scenes
+    from lightmetrica_b200.scene import (AreaLight, ConstantEnvironmentLight, DiffuseBSDF, Primitive, Primitives,
+                                         TriangleMesh)
+    prims = Primitives()
+    V, F = scenes.icosphere(level)
+    prims.add(Primitive(mesh=TriangleMesh((V * 0.5 + [0.0, 3.0, 0.0]).astype(np.float32), F, V.copy()),
+                        bsdf=DiffuseBSDF((0.0, 0.0, 0.0)), light=AreaLight((40.0, 36.0, 30.0))))
+    qv = np.array([[-2, 1, -2], [1, 1, -2], [1, 1.5, 1], [-2, 1.5, 1]], dtype=np.float32)
+    qn = np.tile(np.array([[0.0, -0.986, 0.164]], dtype=np.float32), (4, 1))
+    prims.add(Primitive(mesh=TriangleMesh(qv, np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint32), qn),
+                        bsdf=DiffuseBSDF((0.0, 0.0, 0.0)), light=AreaLight((5.0, 6.0, 7.0))))
+    prims.environment_light = ConstantEnvironmentLight((0.5, 0.5, 0.5))
+    prims.camera = PerspectiveCamera(fovy=45.0, eye=(0.0, 2.0, 6.0), center=(0.0, 1.0, 0.0), up=(0, 1, 0),
+                                     film=HDRBitmapFilm(32, 32))
+    s = Scene("bvh")
+    s.load(prims)
+    s.configure({})
+    s.build()
+    return prims, s
+
+
+@pytest.mark.parametrize("level", [1, 5], ids=["scanned_guide_ranges", "halved_guide_ranges"])
+def test_light_sample_matches_oracle(cuda, level):
+    """Scene::SampleLightSelection + SamplePosition: light choice, position,
+    normal and pdf against the FP64 restatement. The device's triangle CDF
+    is float: where u1 lies within its rounding of a boundary (a fraction
+    ~1e-3 or less of the samples here) it may pick the neighbouring
+    triangle; all other samples agree to float rounding."""
+    prims, scene = light_scene(level)
+    u = np.random.default_rng(5 + level).uniform(size=(200000, 2)).astype(np.float32)
+    got = C.light_sample(scene, u)
+    want, wl = oracle.light_sample(prims, u)
+    np.testing.assert_array_equal(got["light"], wl)
+    assert set(np.unique(wl)) == {0, 1, 2}                       # both area lights and the environment
+    np.testing.assert_allclose(got["pdf"], want[:, 6], rtol=2e-6)
+    d = np.linalg.norm(got["position"] - want[:, :3], axis=1)
+    scale = np.linalg.norm(want[:, :3], axis=1) + 1.0
+    close = d < 2e-5 * scale
+    assert close.mean() > 0.998, close.mean()
+    # The normal is the cross product of two float edge vectors: on the
+    # level-5 sphere the edges (~0.016) are differences of coordinates near 3,
+    # so each carries ~3e-8 * 3 / 0.016 ~ 1e-5 relative rounding.
+    nz = np.linalg.norm(want[:, 3:6], axis=1) > 0
+    np.testing.assert_allclose(got["normal"][close & nz], want[close & nz, 3:6], atol=1e-4)
+    scene.close()
