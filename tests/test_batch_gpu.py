@@ -113,6 +113,33 @@ def test_batch_configurations_agree(cuda, config):
     batch.close()
 
 
+def _shifted(prims, offset):
+    """The same scene moved by `offset` (geometry by its primitives'
+    transforms, and the camera)."""
+    import dataclasses
+    M = np.eye(4)
+    M[:3, 3] = offset
+    moved = dataclasses.replace(prims, primitives=[dataclasses.replace(p, transform=M) for p in prims.primitives])
+    cam = prims.camera
+    moved.camera = dataclasses.replace(cam, eye=tuple(np.add(cam.eye, offset)), center=tuple(np.add(cam.center, offset)))
+    return moved
+
+
+@pytest.mark.parametrize("layout", ["bvh", "qbvh"])
+@pytest.mark.parametrize("offset", [(100.0, -70.0, 130.0), (1000.0, -700.0, 1300.0)], ids=["100", "1000"])
+def test_batch_far_from_origin(cuda, offset, layout):
+    """Far from the origin the coordinates' float spacing grows (1.2e-4 at
+    1,300): the batch's walks must still find exactly the one-scene
+    renderer's hits."""
+    items = [(_shifted(scenes.cornell_box(48, 48, variant="mixed"), offset), renderer("pt.mis", 3, 9, 3), 48 * 48 * 16)]
+    built = [build(p) for p, _, _ in items]
+    want = plain_films(built, items)
+    batch = SceneBatch(built)
+    batch.configure(layout=layout)
+    assert_same(batch_films(batch, items), want)
+    batch.close()
+
+
 @pytest.mark.parametrize("mode", ["waves", "stream", "overlap"])
 def test_batch_unbounded_depth_tail(cuda, mode):
     """max_path_vertices = -1 (Russian roulette only): in wave mode the graph
