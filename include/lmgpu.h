@@ -52,7 +52,11 @@ enum {
 enum {
     LMGPU_LAYOUT_BVH2 = 0,   /* binary, children-in-parent 64 B nodes */
     LMGPU_LAYOUT_BVH4 = 1,   /* 4-wide collapse of the same tree, 128 B nodes */
-    LMGPU_LAYOUT_NAIVE = 2   /* brute force over all triangles (tiny scenes) */
+    LMGPU_LAYOUT_NAIVE = 2,  /* brute force over all triangles (tiny scenes) */
+    LMGPU_LAYOUT_BVH2Q = 3,  /* batch renders only: the binary render tree with 48 B nodes whose child
+                                boxes are 16-bit planes on a per-node grid (boxes only grow) */
+    LMGPU_LAYOUT_BVH2_QSHADOW = 4   /* batch renders only: float binary nodes for bounce rays,
+                                       quantised ones (LMGPU_LAYOUT_BVH2Q) for shadow rays */
 };
 
 /* BSDFs (reference diffuse.cpp, mirror.cpp, plugin.diffusemirror). */
@@ -334,7 +338,7 @@ enum {
 };
 
 typedef struct LmgpuBatchConfig {
-    int32_t layout;               /* LMGPU_LAYOUT_BVH2 or LMGPU_LAYOUT_BVH4 for every scene */
+    int32_t layout;               /* LMGPU_LAYOUT_BVH2, _BVH4, _BVH2Q or _BVH2_QSHADOW for every scene */
     int32_t wave_paths;           /* paths in flight: the capacity of the ray and shadow queues
                                      (per pool), in [1024, 2^27] */
     int32_t shade_blocks_per_sm;  /* grid of the shading kernel (blocks of 128 threads per SM) */

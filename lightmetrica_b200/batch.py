@@ -25,7 +25,11 @@ import numpy as np
 from . import native as N
 from .render import Renderer
 
-LAYOUTS = {"bvh": N.LAYOUT_BVH2, "qbvh": N.LAYOUT_BVH4}
+# "bvh": binary float nodes, "qbvh": 4-wide, "bvh_q16": binary nodes with
+# 16-bit quantised child boxes, "bvh_qshadow": float nodes for bounce rays
+# and quantised ones for shadow rays (the last two: batch renders only).
+LAYOUTS = {"bvh": N.LAYOUT_BVH2, "qbvh": N.LAYOUT_BVH4, "bvh_q16": N.LAYOUT_BVH2Q,
+           "bvh_qshadow": N.LAYOUT_BVH2_QSHADOW}
 MODES = {"waves": N.BATCH_WAVES, "stream": N.BATCH_STREAM, "overlap": N.BATCH_OVERLAP}
 
 
@@ -56,7 +60,7 @@ class SceneBatch:
         N.check(N.lib().lmgpu_batch_get_config(self.handle, ctypes.byref(c)))
         if layout is not None:
             if layout not in LAYOUTS:
-                raise ValueError("layout must be 'bvh' or 'qbvh'")
+                raise ValueError("layout must be one of " + ", ".join(LAYOUTS))
             c.layout = LAYOUTS[layout]
         if wave_paths is not None:
             c.wave_paths = int(wave_paths)

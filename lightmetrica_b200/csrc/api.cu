@@ -423,6 +423,13 @@ int create_impl(const LmgpuSceneDesc* desc, LmgpuScene** out)
         r.stack_cap = 2 * b.rmax_depth + 4;
         if (desc->max_stack_entries > 0 && desc->max_stack_entries < r.stack_cap) r.stack_cap = desc->max_stack_entries;
     }
+    // The quantised copy of the binary tree renders traverse (batch layout
+    // LMGPU_LAYOUT_BVH2Q); rays start in the scene's bounds or at the camera.
+    if (desc->layout != LMGPU_LAYOUT_NAIVE && b.num_tris > 0) {
+        const std::vector<Bvh2QNode> qn = quantize_bvh2(render_tree ? b.rbvh2 : b.bvh2, b.bounds,
+                                                        cam.valid ? cam.position : nullptr);
+        up(qn, &s->rdev.bvh2q);
+    }
     if (rc != LMGPU_OK) { lmgpu_scene_destroy(s); return rc; }
 
     // Scratch: status word and the persistent kernels' work counter.

@@ -234,6 +234,13 @@ __global__ void k_stream_plan(StreamCtl* ctl, uint32_t* counters, int q, unsigne
 
 // ------------------------------------------------------- wave builder ----
 
+// Kernel layout of each walk: LMGPU_LAYOUT_BVH2_QSHADOW traces bounce rays
+// through the float binary nodes and shadow rays through the quantised ones.
+constexpr int walk_layout(int layout, bool any_hit)
+{
+    return layout == LMGPU_LAYOUT_BVH2_QSHADOW ? (any_hit ? LMGPU_LAYOUT_BVH2Q : LMGPU_LAYOUT_BVH2) : layout;
+}
+
 // Launches one persistent traversal of `io`. During a measurement render
 // (b->prof) the launch is bracketed by CUDA events and, when counting, runs
 // the counting instantiation of the same kernel.
@@ -243,7 +250,7 @@ void launch_traversal(const LmgpuBatch* b, int blocks, const DeviceScene& proto,
 {
     TraceProfileRun* p = b->prof;
     if (!p) {
-        k_trace_persistent<LAYOUT, STACK, ANY_HIT, IO><<<blocks, 128, 0, s>>>(proto, io, b->d_status, work, nullptr);
+        k_trace_persistent<walk_layout(LAYOUT, ANY_HIT), STACK, ANY_HIT, IO><<<blocks, 128, 0, s>>>(proto, io, b->d_status, work, nullptr);
         return;
     }
     cudaEvent_t e[2] = { nullptr, nullptr };
@@ -251,10 +258,10 @@ void launch_traversal(const LmgpuBatch* b, int blocks, const DeviceScene& proto,
         if (p->error == cudaSuccess) p->error = cudaEventCreate(&x);
     if (p->error == cudaSuccess) p->error = cudaEventRecord(e[0], s);
     if (p->count)
-        k_trace_persistent<LAYOUT, STACK, ANY_HIT, IO, true><<<blocks, 128, 0, s>>>(
+        k_trace_persistent<walk_layout(LAYOUT, ANY_HIT), STACK, ANY_HIT, IO, true><<<blocks, 128, 0, s>>>(
             proto, io, b->d_status, work, p->d_counts + (ANY_HIT ? 2 : 0));
     else
-        k_trace_persistent<LAYOUT, STACK, ANY_HIT, IO><<<blocks, 128, 0, s>>>(proto, io, b->d_status, work, nullptr);
+        k_trace_persistent<walk_layout(LAYOUT, ANY_HIT), STACK, ANY_HIT, IO><<<blocks, 128, 0, s>>>(proto, io, b->d_status, work, nullptr);
     if (p->error == cudaSuccess) p->error = cudaEventRecord(e[1], s);
     for (cudaEvent_t x : e)
         if (x) p->events.push_back(x);
@@ -336,8 +343,8 @@ struct Wave {
 
     static void warm(Launch& L)
     {
-        L.trace_blocks = resident_blocks(k_trace_persistent<LAYOUT, STACK, false, PathRayIO<true>>);
-        L.shadow_blocks = resident_blocks(k_trace_persistent<LAYOUT, STACK, true, ShadowIO<FilmCtx>>);
+        L.trace_blocks = resident_blocks(k_trace_persistent<walk_layout(LAYOUT, false), STACK, false, PathRayIO<true>>);
+        L.shadow_blocks = resident_blocks(k_trace_persistent<walk_layout(LAYOUT, true), STACK, true, ShadowIO<FilmCtx>>);
     }
 };
 
@@ -377,8 +384,8 @@ struct Stream {
 
     static void warm(Launch& L)
     {
-        L.trace_blocks = resident_blocks(k_trace_persistent<LAYOUT, STACK, false, PathRayIO<true>>);
-        L.shadow_blocks = resident_blocks(k_trace_persistent<LAYOUT, STACK, true, ShadowIO<FilmCtx>>);
+        L.trace_blocks = resident_blocks(k_trace_persistent<walk_layout(LAYOUT, false), STACK, false, PathRayIO<true>>);
+        L.shadow_blocks = resident_blocks(k_trace_persistent<walk_layout(LAYOUT, true), STACK, true, ShadowIO<FilmCtx>>);
     }
 };
 
@@ -742,17 +749,24 @@ int run_waves(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_t&
     return LMGPU_OK;
 }
 
+template <int TECH, class F, int LAYOUT>
+int dispatch_stack(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_t& waves)
+{
+    switch (pl.stack) {
+    case 64: return run_waves<TECH, F, LAYOUT, 64>(b, pl, P, s, waves);
+    case 128: return run_waves<TECH, F, LAYOUT, 128>(b, pl, P, s, waves);
+    default: return run_waves<TECH, F, LAYOUT, 256>(b, pl, P, s, waves);
+    }
+}
+
 template <int TECH, class F>
 int dispatch_layout(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int64_t& waves)
 {
-    const bool bvh4 = b->cfg.layout == LMGPU_LAYOUT_BVH4;
-    switch (pl.stack) {
-    case 64: return bvh4 ? run_waves<TECH, F, LMGPU_LAYOUT_BVH4, 64>(b, pl, P, s, waves)
-                         : run_waves<TECH, F, LMGPU_LAYOUT_BVH2, 64>(b, pl, P, s, waves);
-    case 128: return bvh4 ? run_waves<TECH, F, LMGPU_LAYOUT_BVH4, 128>(b, pl, P, s, waves)
-                          : run_waves<TECH, F, LMGPU_LAYOUT_BVH2, 128>(b, pl, P, s, waves);
-    default: return bvh4 ? run_waves<TECH, F, LMGPU_LAYOUT_BVH4, 256>(b, pl, P, s, waves)
-                         : run_waves<TECH, F, LMGPU_LAYOUT_BVH2, 256>(b, pl, P, s, waves);
+    switch (b->cfg.layout) {
+    case LMGPU_LAYOUT_BVH4: return dispatch_stack<TECH, F, LMGPU_LAYOUT_BVH4>(b, pl, P, s, waves);
+    case LMGPU_LAYOUT_BVH2Q: return dispatch_stack<TECH, F, LMGPU_LAYOUT_BVH2Q>(b, pl, P, s, waves);
+    case LMGPU_LAYOUT_BVH2_QSHADOW: return dispatch_stack<TECH, F, LMGPU_LAYOUT_BVH2_QSHADOW>(b, pl, P, s, waves);
+    default: return dispatch_stack<TECH, F, LMGPU_LAYOUT_BVH2>(b, pl, P, s, waves);
     }
 }
 
@@ -768,8 +782,9 @@ int dispatch_tech(LmgpuBatch* b, const Plan& pl, int64_t P, cudaStream_t s, int6
 
 int check_config(const LmgpuBatchConfig& c)
 {
-    if (c.layout != LMGPU_LAYOUT_BVH2 && c.layout != LMGPU_LAYOUT_BVH4)
-        return fail(LMGPU_ERR_INVALID, "batch layout must be LMGPU_LAYOUT_BVH2 or LMGPU_LAYOUT_BVH4");
+    if (c.layout != LMGPU_LAYOUT_BVH2 && c.layout != LMGPU_LAYOUT_BVH4 && c.layout != LMGPU_LAYOUT_BVH2Q &&
+        c.layout != LMGPU_LAYOUT_BVH2_QSHADOW)
+        return fail(LMGPU_ERR_INVALID, "batch layout must be LMGPU_LAYOUT_BVH2, _BVH4, _BVH2Q or _BVH2_QSHADOW");
     if (c.wave_paths < 1024 || c.wave_paths > (1 << 27)) return fail(LMGPU_ERR_INVALID, "wave_paths must be in [1024, 2^27]");
     if (c.shade_blocks_per_sm < 1 || c.shade_blocks_per_sm > 64) return fail(LMGPU_ERR_INVALID, "shade_blocks_per_sm must be in [1, 64]");
     if (c.mode != LMGPU_BATCH_WAVES && c.mode != LMGPU_BATCH_STREAM && c.mode != LMGPU_BATCH_OVERLAP)
@@ -1121,7 +1136,7 @@ int lmgpu_batch_autotune(LmgpuBatch* b, const LmgpuRenderParams* params, double 
         double t;
         if ((rc = trial(c, t)) == LMGPU_OK && t < best_t) { best = c; best_t = t; }
     }
-    const int layouts[] = { LMGPU_LAYOUT_BVH2, LMGPU_LAYOUT_BVH4 };
+    const int layouts[] = { LMGPU_LAYOUT_BVH2, LMGPU_LAYOUT_BVH4, LMGPU_LAYOUT_BVH2Q, LMGPU_LAYOUT_BVH2_QSHADOW };
     const int waves[] = { 1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25, 1 << 26, 1 << 27 };
     const int grids[] = { 4, 8, 16 };
     for (int l : layouts) {

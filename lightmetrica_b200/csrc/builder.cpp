@@ -18,6 +18,7 @@
 #include <cfloat>
 #include <cstring>
 #include <functional>
+#include <limits>
 #include <thread>
 
 namespace lmgpu {
@@ -403,6 +404,51 @@ struct RenderBuilder {
 };
 
 }  // namespace
+
+std::vector<Bvh2QNode> quantize_bvh2(const std::vector<Bvh2Node>& nodes, const HostAabb& bounds,
+                                     const float* extra)
+{
+    double M = 0.0;
+    for (int c = 0; c < 3; c++) {
+        M = std::max(M, (double)std::fabs(bounds.mn[c]));
+        M = std::max(M, (double)std::fabs(bounds.mx[c]));
+        if (extra) M = std::max(M, (double)std::fabs(extra[c]));
+    }
+    // 16 ulps of the largest magnitude a ray origin or a plane takes
+    const double min_step = 16.0 * (M > 0.0 ? std::ldexp(1.0, std::ilogb(M) - 23) : std::ldexp(1.0, -126));
+    std::vector<Bvh2QNode> out(nodes.size());
+    for (size_t i = 0; i < nodes.size(); i++) {
+        const Bvh2Node& n = nodes[i];
+        const float* ax[3] = { n.bx, n.by, n.bz };
+        Bvh2QNode& o = out[i];
+        uint32_t exps = (uint32_t)(n.axis & 0xff) << 24;
+        for (int k = 0; k < 3; k++) {
+            const double lo = std::min(ax[k][0], ax[k][2]), hi = std::max(ax[k][1], ax[k][3]);
+            // 65,520 steps cover the box, its two-step margins and the
+            // origin's rounding; a power of two, so q * step is exact.
+            const double need = std::max(min_step, (hi - lo) / 65520.0);
+            int E = std::ilogb(need);
+            if (std::ldexp(1.0, E) < need) E++;
+            E = std::min(std::max(E, -126), 127);
+            const double step = std::ldexp(1.0, E);
+            const double od = lo - 2.0 * step;
+            float of = (float)od;
+            if ((double)of > od) of = std::nextafter(of, -std::numeric_limits<float>::infinity());
+            o.origin[k] = of;
+            for (int c = 0; c < 2; c++) {
+                const double clo = ax[k][2 * c], chi = ax[k][2 * c + 1];
+                const double qlo = std::max(0.0, std::floor((clo - (double)of) / step) - 2.0);
+                const double qhi = std::min(65535.0, std::ceil((chi - (double)of) / step) + 2.0);
+                o.q[2 * k + c] = (uint32_t)qlo | ((uint32_t)qhi << 16);
+            }
+            exps |= (uint32_t)(E + 127) << (8 * k);
+        }
+        o.exps = exps;
+        o.left = n.left;
+        o.right = n.right;
+    }
+    return out;
+}
 
 void build_render_tree(BuiltScene& s, int threads)
 {

@@ -75,6 +75,14 @@ struct PrimitiveInput {
     const float* transform;   // 16 floats column-major or nullptr
 };
 
+// The quantised copy of a binary tree (same node order and references) for
+// rays that start within `bounds` (or at `extra`, a camera position): the
+// grid step of an axis is a power of two no finer than 16 float ulps of the
+// largest coordinate magnitude, so the decode's rounding stays below the
+// two-step margin around every box.
+std::vector<Bvh2QNode> quantize_bvh2(const std::vector<Bvh2Node>& nodes, const HostAabb& bounds,
+                                     const float* extra);
+
 // Builds everything; returns an empty string on success, else an error.
 std::string build_scene(const std::vector<PrimitiveInput>& prims, int threads, bool want_bvh,
                         BuiltScene& out);

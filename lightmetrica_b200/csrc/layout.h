@@ -48,6 +48,20 @@ struct alignas(16) Bvh4Node {
 static_assert(sizeof(Bvh4Node) == 128, "Bvh4Node is 128 B");
 constexpr int32_t BVH4_EMPTY = 0x7fffffff;
 
+// Quantised binary node (LMGPU_LAYOUT_BVH2Q, render trees only): the same
+// tree as Bvh2Node with each child box on a per-node grid. Axis k's planes
+// sit at origin[k] + q * 2^(e_k - 127) for 16-bit q, where e_k is byte k of
+// `exps`. quantize_bvh2 (builder.cpp) chooses grid and q so that every
+// quantised box contains its child's float box with a margin of two grid
+// steps. 48 B: three 16-byte loads per visit instead of four.
+struct alignas(16) Bvh2QNode {
+    float origin[3];
+    uint32_t exps;         // e_x | e_y << 8 | e_z << 16 | split axis << 24
+    uint32_t q[6];         // axis k: q[2k] left child, q[2k + 1] right child, each lo | hi << 16
+    int32_t left, right;   // child references as in Bvh2Node
+};
+static_assert(sizeof(Bvh2QNode) == 48, "Bvh2QNode is 48 B");
+
 struct alignas(16) TriRecord {
     uint32_t k_flags;      // TriAccel::k | TRI_LAST_IN_LEAF
     float n_u, n_v, n_d;

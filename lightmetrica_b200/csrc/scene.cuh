@@ -56,6 +56,7 @@ struct DeviceScene {
     float root_box[6];     // lo.xyz, hi.xyz
     const Bvh2Node* bvh2;
     const Bvh4Node* bvh4;
+    const Bvh2QNode* bvh2q;       // render view: the quantised copy of bvh2 (LMGPU_LAYOUT_BVH2Q)
     const TriRecord* tris;        // leaf order
     const TriRecord* tris_by_id;  // TriAccel order (naive layout)
     int64_t num_tris;

@@ -169,18 +169,24 @@ __device__ __forceinline__ void plane_pair_fma(float lo, float hi, float inv, fl
         : "=f"(a), "=f"(b) : "f"(lo), "f"(hi), "f"(inv), "f"(noinv));
 }
 
+// Entry and exit of a box from its six plane distances (x lo, x hi, y lo, ...).
+__device__ __forceinline__ bool slab_interval(const TraversalRay& r, const float* t, float& t_enter)
+{
+    const float tn = fmaxf(fmaxf(fminf(t[0], t[1]), fminf(t[2], t[3])), fminf(t[4], t[5]));
+    const float tf = fminf(fminf(fmaxf(t[0], t[1]), fmaxf(t[2], t[3])), fmaxf(t[4], t[5]));
+    t_enter = tn;
+    return tn <= tf && tf > r.tmin;
+}
+
 __device__ __forceinline__ bool slab_render(const TraversalRay& r,
                                             float lox, float hix, float loy, float hiy,
                                             float loz, float hiz, float& t_enter)
 {
-    float ax, bx, ay, by, az, bz;
-    plane_pair_fma(lox, hix, r.inv_min[0], r.inv_max[0], ax, bx);
-    plane_pair_fma(loy, hiy, r.inv_min[1], r.inv_max[1], ay, by);
-    plane_pair_fma(loz, hiz, r.inv_min[2], r.inv_max[2], az, bz);
-    const float tn = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fminf(az, bz));
-    const float tf = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
-    t_enter = tn;
-    return tn <= tf && tf > r.tmin;
+    float t[6];
+    plane_pair_fma(lox, hix, r.inv_min[0], r.inv_max[0], t[0], t[1]);
+    plane_pair_fma(loy, hiy, r.inv_min[1], r.inv_max[1], t[2], t[3]);
+    plane_pair_fma(loz, hiz, r.inv_min[2], r.inv_max[2], t[4], t[5]);
+    return slab_interval(r, t, t_enter);
 }
 
 // Both child boxes of a binary node (render rays or the exact test).
@@ -389,6 +395,57 @@ __device__ __forceinline__ void trav_begin(TravState& ts, int32_t root_ref, cons
 #define LMGPU_TRACE_SPECULATIVE 1
 #endif
 
+// Slab tests of both children of binary node `ref`: pass bits and entry
+// distances (left: pl, tl; right: pr, tr); returns (left, right, split axis).
+template <bool RENDER>
+__device__ __forceinline__ int3 node_children(const Bvh2Node* __restrict__ nodes, int32_t ref, const TraversalRay& r,
+                                              bool& pl, float& tl, bool& pr, float& tr)
+{
+    const float4* np = reinterpret_cast<const float4*>(nodes + ref);
+    const float4 bx = __ldg(np), by = __ldg(np + 1), bz = __ldg(np + 2);
+    const int4 meta = __ldg(reinterpret_cast<const int4*>(np + 3));
+    slab_pair<RENDER>(r, bx, by, bz, pl, tl, pr, tr);
+    return make_int3(meta.x, meta.y, meta.z);
+}
+
+// The same for a quantised node (render rays). A plane at grid index q of
+// axis k lies at origin_k + q * step_k, so its distance along the ray is
+// q * (step_k / d_k) + (origin_k - o_k) / d_k: one multiply-add per plane,
+// two planes per packed fma.rn.f32x2 as in slab_render. q becomes a float
+// as 2^23 + q (its 16 bits under the exponent of 2^23, one byte permute);
+// the 2^23 * step_k / d_k this adds is taken off the per-axis bias. That
+// subtraction rounds at about half a grid step along the axis, inside the
+// two-step margin quantize_bvh2 leaves around every box.
+__device__ __forceinline__ float grid_plane(uint32_t word, bool hi)
+{
+    return __uint_as_float(__byte_perm(word, 0x4b00u, hi ? 0x5432u : 0x5410u));
+}
+template <bool RENDER>
+__device__ __forceinline__ int3 node_children(const Bvh2QNode* __restrict__ nodes, int32_t ref, const TraversalRay& r,
+                                              bool& pl, float& tl, bool& pr, float& tr)
+{
+    static_assert(RENDER && LMGPU_RENDER_FMA_SLAB, "quantised nodes serve render rays only");
+    const uint4* np = reinterpret_cast<const uint4*>(nodes + ref);
+    const uint4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2);
+    const uint32_t words[6] = { b.x, b.y, b.z, b.w, c.x, c.y };
+    const float origin[3] = { __uint_as_float(a.x), __uint_as_float(a.y), __uint_as_float(a.z) };
+    float t[2][6];   // [child][lo/hi of x, y, z]
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const float step = __uint_as_float(((a.w >> (8 * k)) & 0xffu) << 23);
+        const float s = step * r.inv_min[k];
+        const float bias = fmaf(-8388608.0f, s, fmaf(origin[k], r.inv_min[k], r.inv_max[k]));
+#pragma unroll
+        for (int ch = 0; ch < 2; ch++) {
+            const uint32_t w = words[2 * k + ch];
+            plane_pair_fma(grid_plane(w, false), grid_plane(w, true), s, bias, t[ch][2 * k], t[ch][2 * k + 1]);
+        }
+    }
+    pl = slab_interval(r, t[0], tl);
+    pr = slab_interval(r, t[1], tr);
+    return make_int3((int)c.z, (int)c.w, (int)(a.w >> 24));
+}
+
 // Child order of render walks: LMGPU_RENDER_NEAR_FIRST 1 visits the child
 // with the nearer entry distance first; 0 the reference's order (right
 // child first iff the ray points down the split axis), which the exact
@@ -405,8 +462,8 @@ __device__ __forceinline__ void trav_begin(TravState& ts, int32_t root_ref, cons
 #define LMGPU_RENDER_ANY_NEAR_FIRST 1
 #endif
 
-template <int EXIT_BELOW = 0, bool RENDER = false, bool SPEC = false, class Stack>
-__device__ __forceinline__ bool bvh2_descend(const Bvh2Node* __restrict__ nodes, TravState& ts, Stack stack,
+template <int EXIT_BELOW = 0, bool RENDER = false, bool SPEC = false, class Node, class Stack>
+__device__ __forceinline__ bool bvh2_descend(const Node* __restrict__ nodes, TravState& ts, Stack stack,
                                              int stack_cap, const TraversalRay& r, TraceStats* st,
                                              bool may_exit = false, int32_t* pend = nullptr)
 {
@@ -420,12 +477,9 @@ __device__ __forceinline__ bool bvh2_descend(const Bvh2Node* __restrict__ nodes,
         if (SPEC && __all_sync(__activemask(), *pend != 0)) break;
         if (EXIT_BELOW > 0 && may_exit && stepped && __popc(__activemask()) < EXIT_BELOW) break;
         stepped = true;
-        const float4* np = reinterpret_cast<const float4*>(nodes + ts.ref);
-        const float4 bx = __ldg(np), by = __ldg(np + 1), bz = __ldg(np + 2);
-        const int4 meta = __ldg(reinterpret_cast<const int4*>(np + 3));
         float tl = 0.f, tr = 0.f;
         bool pl, pr;
-        slab_pair<RENDER>(r, bx, by, bz, pl, tl, pr, tr);
+        const int3 meta = node_children<RENDER>(nodes, ts.ref, r, pl, tl, pr, tr);
         const bool right_first = (RENDER && LMGPU_RENDER_NEAR_FIRST) ? (pr && (!pl || tr < tl))
                                                                      : bool((r.neg >> meta.z) & 1u);
         const int32_t near_ref = right_first ? meta.y : meta.x;
@@ -515,8 +569,8 @@ __device__ __forceinline__ void pop_any(TravState& ts, Stack stack)
 // first iff the ray direction is negative on the split axis; render walks:
 // LMGPU_RENDER_ANY_NEAR_FIRST). Returns false on stack overflow;
 // EXIT_BELOW / may_exit as in bvh2_descend.
-template <int EXIT_BELOW = 0, bool RENDER = false, bool SPEC = false, class Stack>
-__device__ __forceinline__ bool bvh2_descend_any(const Bvh2Node* __restrict__ nodes, TravState& ts, Stack stack,
+template <int EXIT_BELOW = 0, bool RENDER = false, bool SPEC = false, class Node, class Stack>
+__device__ __forceinline__ bool bvh2_descend_any(const Node* __restrict__ nodes, TravState& ts, Stack stack,
                                                  int stack_cap, const TraversalRay& r, TraceStats* st,
                                                  bool may_exit = false, int32_t* pend = nullptr)
 {
@@ -530,12 +584,9 @@ __device__ __forceinline__ bool bvh2_descend_any(const Bvh2Node* __restrict__ no
         if (SPEC && __all_sync(__activemask(), *pend != 0)) break;
         if (EXIT_BELOW > 0 && may_exit && stepped && __popc(__activemask()) < EXIT_BELOW) break;
         stepped = true;
-        const float4* np = reinterpret_cast<const float4*>(nodes + ts.ref);
-        const float4 bx = __ldg(np), by = __ldg(np + 1), bz = __ldg(np + 2);
-        const int4 meta = __ldg(reinterpret_cast<const int4*>(np + 3));
         float tl = 0.f, tr = 0.f;
         bool pl, pr;
-        slab_pair<RENDER>(r, bx, by, bz, pl, tl, pr, tr);
+        const int3 meta = node_children<RENDER>(nodes, ts.ref, r, pl, tl, pr, tr);
         if (st) st->nodes += 2;
         const bool hl = pl && tl < r.tmax, hr = pr && tr < r.tmax;
         if (hl && hr) {

@@ -79,6 +79,7 @@ struct exit_below<IO, std::void_t<decltype(IO::EXIT_BELOW)>> : std::integral_con
 struct LaneScene {
     const Bvh2Node* bvh2;
     const Bvh4Node* bvh4;
+    const Bvh2QNode* bvh2q;
     const TriRecord* tris;
 };
 
@@ -87,10 +88,16 @@ template <int LAYOUT, int EXIT, bool RENDER, bool SPEC, class Stack>
 __device__ __forceinline__ bool descend(const LaneScene& s, TravState& ts, Stack stack, int cap,
                                         const TraversalRay& r, bool may_exit, TraceStats* st, int32_t* pend)
 {
-    if (LAYOUT == LMGPU_LAYOUT_BVH2)
+    if constexpr (LAYOUT == LMGPU_LAYOUT_BVH2)
         return bvh2_descend<EXIT, RENDER, SPEC>(s.bvh2, ts, stack, cap, r, st, may_exit, pend);
-    return bvh4_descend<EXIT, RENDER>(s.bvh4, ts, stack, cap, r, st, may_exit);
+    else if constexpr (LAYOUT == LMGPU_LAYOUT_BVH2Q)
+        return bvh2_descend<EXIT, RENDER, SPEC>(s.bvh2q, ts, stack, cap, r, st, may_exit, pend);
+    else
+        return bvh4_descend<EXIT, RENDER>(s.bvh4, ts, stack, cap, r, st, may_exit);
 }
+
+// Binary layouts (float or quantised nodes) share the walks and stacks.
+constexpr bool binary_layout(int layout) { return layout == LMGPU_LAYOUT_BVH2 || layout == LMGPU_LAYOUT_BVH2Q; }
 
 // Adds each lane's counts to counts[0] (binary-node slab tests; four per
 // 4-wide node) and counts[1] (TriAccel tests); the whole warp calls it.
@@ -128,7 +135,7 @@ __device__ __forceinline__ void add_trace_stats(const TraceStats& st, unsigned l
 // LMGPU_TRACE_SPECULATIVE=2): each round a lane tests at most one leaf, the
 // one it postponed, and the warp's leaf tests fall in the same round.
 template <int LAYOUT, bool ANY_HIT>
-struct RefStackWalk : std::bool_constant<LMGPU_TRACE_ANYHIT_WALK && ANY_HIT && LAYOUT == LMGPU_LAYOUT_BVH2> {};
+struct RefStackWalk : std::bool_constant<LMGPU_TRACE_ANYHIT_WALK && ANY_HIT && binary_layout(LAYOUT)> {};
 
 template <int LAYOUT, int STACK, bool ANY_HIT, class IO, bool COUNT = false>
 __global__ void __launch_bounds__(128, min_blocks<IO>::value)
@@ -138,7 +145,7 @@ k_trace_persistent(const DeviceScene s, const IO io, int32_t* status, unsigned l
     constexpr unsigned FULL = 0xffffffffu;
     constexpr bool REFS = RefStackWalk<LAYOUT, ANY_HIT>::value;
     constexpr bool RENDER = render_rays<IO>::value;
-    constexpr bool SPEC = RENDER && LAYOUT == LMGPU_LAYOUT_BVH2 &&
+    constexpr bool SPEC = RENDER && binary_layout(LAYOUT) &&
                           (REFS ? LMGPU_TRACE_SPECULATIVE >= 1 : LMGPU_TRACE_SPECULATIVE >= 2);
 #if LMGPU_TRACE_SHARED_STACK > 0
     // The shared part takes the same bytes either way: twice as many
@@ -155,9 +162,9 @@ k_trace_persistent(const DeviceScene s, const IO io, int32_t* status, unsigned l
 #endif
     const int64_t n = io.count();
     const unsigned lane = threadIdx.x & 31u;
-    const int32_t root = LAYOUT == LMGPU_LAYOUT_BVH2 ? s.root_ref : s.root_ref4;
+    const int32_t root = binary_layout(LAYOUT) ? s.root_ref : s.root_ref4;
     const int cap = s.stack_cap < STACK ? s.stack_cap : STACK;
-    LaneScene ls{ s.bvh2, s.bvh4, s.tris };
+    LaneScene ls{ s.bvh2, s.bvh4, s.bvh2q, s.tris };
     TraceStats stats{ 0, 0 };
     TraceStats* const st = COUNT ? &stats : nullptr;
     TraversalRay r;
@@ -187,9 +194,10 @@ k_trace_persistent(const DeviceScene s, const IO io, int32_t* status, unsigned l
                         const DeviceScene& rs = io.ray_scene(idx);
                         ls.bvh2 = rs.bvh2;
                         ls.bvh4 = rs.bvh4;
+                        ls.bvh2q = rs.bvh2q;
                         ls.tris = rs.tris;
                         if (rs.num_tris > 0)
-                            trav_begin<RENDER>(ts, LAYOUT == LMGPU_LAYOUT_BVH2 ? rs.root_ref : rs.root_ref4, rs.root_box, r, st);
+                            trav_begin<RENDER>(ts, binary_layout(LAYOUT) ? rs.root_ref : rs.root_ref4, rs.root_box, r, st);
                     } else {
                         trav_begin<RENDER>(ts, root, s.root_box, r, st);
                     }
@@ -202,7 +210,10 @@ k_trace_persistent(const DeviceScene s, const IO io, int32_t* status, unsigned l
         if (ts.ref != REF_DONE || pend != 0) {
             bool ok = true;
             if (ts.ref != REF_DONE) {
-                if constexpr (REFS)
+                if constexpr (REFS && LAYOUT == LMGPU_LAYOUT_BVH2Q)
+                    ok = bvh2_descend_any<exit_below<IO>::value, RENDER, SPEC>(ls.bvh2q, ts, stack, cap, r, st,
+                                                                             !exhausted, &pend);
+                else if constexpr (REFS)
                     ok = bvh2_descend_any<exit_below<IO>::value, RENDER, SPEC>(ls.bvh2, ts, stack, cap, r, st,
                                                                              !exhausted, &pend);
                 else
@@ -227,7 +238,7 @@ k_trace_persistent(const DeviceScene s, const IO io, int32_t* status, unsigned l
                 // nodes count their four slab tests when fetched)
                 if (trace_leaf<ANY_HIT, RENDER>(ls.tris, ~ts.ref, r, h, st) && ANY_HIT) ts.ref = REF_DONE;
                 else if constexpr (REFS) pop_any(ts, stack);
-                else pop_next(ts, stack, r, LAYOUT == LMGPU_LAYOUT_BVH2 ? st : nullptr);
+                else pop_next(ts, stack, r, binary_layout(LAYOUT) ? st : nullptr);
             }
             if (ts.ref == REF_DONE) io.store(idx, h, r);
         }

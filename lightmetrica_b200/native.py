@@ -38,7 +38,7 @@ STATUS_NAMES = {OK: "OK", ERR_INVALID: "INVALID", ERR_OOM: "OOM", ERR_CUDA: "CUD
                 ERR_STACK_OVERFLOW: "STACK_OVERFLOW", ERR_QUEUE_OVERFLOW: "QUEUE_OVERFLOW",
                 ERR_TIMEOUT: "TIMEOUT", ERR_UNSUPPORTED: "UNSUPPORTED", ERR_BOUNDS: "BOUNDS"}
 
-LAYOUT_BVH2, LAYOUT_BVH4, LAYOUT_NAIVE = 0, 1, 2
+LAYOUT_BVH2, LAYOUT_BVH4, LAYOUT_NAIVE, LAYOUT_BVH2Q, LAYOUT_BVH2_QSHADOW = 0, 1, 2, 3, 4
 RENDER_TREE_SAH, RENDER_TREE_REFERENCE = 0, 1
 BSDF_DIFFUSE, BSDF_MIRROR, BSDF_DIFFUSE_MIRROR, BSDF_BLACK = 0, 1, 2, 3
 RENDER_PT, RENDER_PT_DIRECT, RENDER_PT_MIS = 0, 1, 2

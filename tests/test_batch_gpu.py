@@ -101,6 +101,10 @@ def test_batch_matches_one_scene_renders(cuda, technique):
     dict(mode="overlap", wave_paths=5000, overlap_bounce=1),    # the whole path loop is the tail
     dict(mode="overlap", wave_paths=6000, overlap_bounce=12),   # split past the last bounce
     dict(mode="overlap", layout="qbvh", wave_paths=4096, overlap_bounce=4, use_graph=False),  # two streams
+    dict(layout="bvh_q16"),                      # quantised nodes: boxes only grow, so the same hits here
+    dict(mode="waves", layout="bvh_q16", wave_paths=10000, use_graph=False),
+    dict(layout="bvh_qshadow"),                  # float nodes for bounce rays, quantised for shadow rays
+    dict(mode="overlap", layout="bvh_qshadow", wave_paths=4096),
 ])
 def test_batch_configurations_agree(cuda, config):
     items = small_set()
@@ -123,6 +127,26 @@ def _shifted(prims, offset):
     cam = prims.camera
     moved.camera = dataclasses.replace(cam, eye=tuple(np.add(cam.eye, offset)), center=tuple(np.add(cam.center, offset)))
     return moved
+
+
+@pytest.mark.parametrize("layout", ["bvh_q16", "bvh_qshadow"])
+def test_quantised_layouts_on_a_deep_tree(cuda, layout):
+    """A 256 x 256-vertex terrain with level-3 spheres (a deep tree of tiny
+    triangles, quantisation steps down to ~1e-6): every quantised box holds
+    its float box, so the walks find the float tree's hits and the films
+    equal the one-scene renderer's. Far from the origin this stops holding
+    exactly (a scene 100 units away differed in 0.26 % of its pixels): the
+    render triangle test's rounding there admits hits just outside a
+    triangle's edges, and the wider quantised boxes let more of those
+    through than the float boxes do."""
+    prims = scenes.terrain_spheres(64, 36, grid=256, spheres=8, ico_level=3)
+    items = [(prims, renderer("pt.mis", 4, 9, 2), 64 * 36 * 8)]
+    built = [build(p) for p, _, _ in items]
+    want = plain_films(built, items)
+    batch = SceneBatch(built)
+    batch.configure(layout=layout)
+    assert_same(batch_films(batch, items), want)
+    batch.close()
 
 
 @pytest.mark.parametrize("layout", ["bvh", "qbvh"])
@@ -199,7 +223,7 @@ def test_batch_autotune_keeps_results(cuda):
     want = plain_films(built, items)
     batch = SceneBatch(built)
     cfg = batch.autotune([r for _, r, _ in items], [n for _, _, n in items], sample_fraction=0.25)
-    assert cfg["layout"] in ("bvh", "qbvh") and cfg["trial_ms"] > 0 and cfg["mode"] in ("waves", "stream", "overlap")
+    assert cfg["layout"] in ("bvh", "qbvh", "bvh_q16", "bvh_qshadow") and cfg["trial_ms"] > 0 and cfg["mode"] in ("waves", "stream", "overlap")
     assert 0 <= cfg["overlap_bounce"] <= 5
     assert cfg["wave_paths"] in (1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25, 1 << 26, 1 << 27)
     assert_same(batch_films(batch, items), want)
