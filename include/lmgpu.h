@@ -406,7 +406,9 @@ int lmgpu_batch_profile(LmgpuBatch* batch, const LmgpuRenderParams* params, void
  * holds four of its waves, eight in overlap mode, or the whole render) under candidate
  * configurations (mode, BVH layout, paths in flight, shading grid, overlap
  * bounce), coordinate by coordinate, keeps the one with the least device
- * time per sample, stores it as the batch's configuration and returns it
+ * time per sample (a candidate must beat the incumbent, which starts as the
+ * batch's configuration, by more than 0.5 %), stores it as the batch's
+ * configuration and returns it
  * with that time scaled to `sample_fraction` of the samples, in ms. Films
  * are scratch memory of the tuner; synchronises. */
 int lmgpu_batch_autotune(LmgpuBatch* batch, const LmgpuRenderParams* params, double sample_fraction,

@@ -1123,6 +1123,11 @@ int lmgpu_batch_autotune(LmgpuBatch* b, const LmgpuRenderParams* params, double 
         ms_per_sample = best / (double)samples;
         return LMGPU_OK;
     };
+    // A candidate replaces the incumbent only if it is more than 0.5 % faster:
+    // trial-to-trial noise is ~0.3 %, and without the margin the descent
+    // drifted from the defaults on ties (for the 1080p frame into waves of
+    // 2^26 paths, 0.3 % slower in the timed frames).
+    auto better = [](double t, double incumbent) { return t < incumbent * 0.995; };
     LmgpuBatchConfig best = start;
     best.use_graph = 1;
     double best_t = 1e30;
@@ -1134,7 +1139,7 @@ int lmgpu_batch_autotune(LmgpuBatch* b, const LmgpuRenderParams* params, double 
         LmgpuBatchConfig c = best;
         c.mode = m;
         double t;
-        if ((rc = trial(c, t)) == LMGPU_OK && t < best_t) { best = c; best_t = t; }
+        if ((rc = trial(c, t)) == LMGPU_OK && better(t, best_t)) { best = c; best_t = t; }
     }
     const int layouts[] = { LMGPU_LAYOUT_BVH2, LMGPU_LAYOUT_BVH4, LMGPU_LAYOUT_BVH2Q, LMGPU_LAYOUT_BVH2_QSHADOW };
     const int waves[] = { 1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25, 1 << 26, 1 << 27 };
@@ -1144,7 +1149,7 @@ int lmgpu_batch_autotune(LmgpuBatch* b, const LmgpuRenderParams* params, double 
         LmgpuBatchConfig c = best;
         c.layout = l;
         double t;
-        if ((rc = trial(c, t)) == LMGPU_OK && t < best_t) { best = c; best_t = t; }
+        if ((rc = trial(c, t)) == LMGPU_OK && better(t, best_t)) { best = c; best_t = t; }
     }
     int64_t largest = 0;
     for (int w : waves) {
@@ -1154,14 +1159,14 @@ int lmgpu_batch_autotune(LmgpuBatch* b, const LmgpuRenderParams* params, double 
         LmgpuBatchConfig c = best;
         c.wave_paths = w;
         double t;
-        if ((rc = trial(c, t)) == LMGPU_OK && t < best_t) { best = c; best_t = t; }
+        if ((rc = trial(c, t)) == LMGPU_OK && better(t, best_t)) { best = c; best_t = t; }
     }
     for (int g : grids) {
         if (rc != LMGPU_OK || g == best.shade_blocks_per_sm) continue;
         LmgpuBatchConfig c = best;
         c.shade_blocks_per_sm = g;
         double t;
-        if ((rc = trial(c, t)) == LMGPU_OK && t < best_t) { best = c; best_t = t; }
+        if ((rc = trial(c, t)) == LMGPU_OK && better(t, best_t)) { best = c; best_t = t; }
     }
     if (best.mode == LMGPU_BATCH_OVERLAP) {
         const int current = best.overlap_bounce > 0 ? best.overlap_bounce : DEFAULT_OVERLAP_BOUNCE;
@@ -1170,7 +1175,7 @@ int lmgpu_batch_autotune(LmgpuBatch* b, const LmgpuRenderParams* params, double 
             LmgpuBatchConfig c = best;
             c.overlap_bounce = t0;
             double t;
-            if ((rc = trial(c, t)) == LMGPU_OK && t < best_t) { best = c; best_t = t; }
+            if ((rc = trial(c, t)) == LMGPU_OK && better(t, best_t)) { best = c; best_t = t; }
         }
     }
     cudaFree(film);
