@@ -54,6 +54,13 @@ NODE_BYTES = 32      # compact binary node (6 f32 + 2 u32), per slab test
 NODE4_BYTES = 128    # 4-wide node, per node fetch (four slab tests)
 TRI_BYTES = 48       # TriAccel record, per triangle test
 RAY_IO_BYTES = 32 + 16
+QNODE_BYTES = 24     # quantised binary node (48 B: grid, 16-bit planes, children), per slab test
+
+
+def node_bytes(layout: str, any_hit: bool) -> int:
+    """Node bytes per slab test of a render walk under the batch layout."""
+    quantised = layout == "bvh_q16" or (layout == "bvh_qshadow" and any_hit)
+    return QNODE_BYTES if quantised else NODE_BYTES
 
 # Headline frame: the full path tracer on the terrain + icospheres scene.
 FRAME_W, FRAME_H = 1920, 1080
@@ -314,12 +321,13 @@ def _batch_launches(cfg, stats, bounces):
     return stats["waves"] * (5 + 4 * bounces) + 1
 
 
-def frame_roofline(prof_count, prof_time):
+def frame_roofline(prof_count, prof_time, layout="bvh"):
     """Roofline of the dominant kernel of the frame, the closest-hit
     traversal of the path queues (and, beside it, the shadow traversal):
     algorithmic bytes (SURVEY d: 32 B ray + 16 B hit + 32 B per binary-node
-    slab test + 48 B per TriAccel test, counted on the same samples by the
-    counting kernel) over the launches' summed device time."""
+    slab test, 24 B for a quantised node, + 48 B per TriAccel test, counted
+    on the same samples by the counting kernel) over the launches' summed
+    device time."""
     peak, peak_kind = measured_peaks()
     out = {}
     for kind in ("closest", "shadow"):
@@ -329,7 +337,7 @@ def frame_roofline(prof_count, prof_time):
             continue
         nb = c["node_tests"] / rays
         tb = c["tri_tests"] / rays
-        bpr = RAY_IO_BYTES + NODE_BYTES * nb + TRI_BYTES * tb
+        bpr = RAY_IO_BYTES + node_bytes(layout, kind == "shadow") * nb + TRI_BYTES * tb
         achieved = bpr * rays / (t["trace_ms"] / 1e3) / 1e9
         out[kind] = {"achieved": round(achieved, 1), "frac": round(achieved / peak, 4),
                      "bytes_per_ray": round(bpr, 2), "node_tests_per_ray": round(nb, 3),
@@ -446,7 +454,7 @@ def run_ours(args):
                "steps": steps, "api": "SceneBatch.render -> lmgpu_batch_render (host film, rescaled)",
                "inputs": "the render parameters of the step (the scene stays resident in HBM)"}
 
-    roofline = frame_roofline(prof_count, prof_time)
+    roofline = frame_roofline(prof_count, prof_time, batch.config["layout"])
     launches = _batch_launches(batch.config, stats, FRAME_MAX_PV - 1) * args.steps
     batch.close()
 
