@@ -77,6 +77,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer passes (profiling runs)")
     ap.add_argument("--no-autotune", action="store_true", help="headline: the batch's default configuration")
+    ap.add_argument("--frame-layout", default=None, choices=["bvh", "qbvh", "bvh_q16", "bvh_qshadow"],
+                    help="headline: this node layout after any tuning (profiling runs)")
     ap.add_argument("--rays-log2", type=int, default=24, help="intersection section: ray batch 2^k")
     ap.add_argument("--render-spp", type=int, default=64, help="spp of the 1080p frame (profiling runs use less)")
     ap.add_argument("--render-frames", type=int, default=3, help="timed frames of the plain-renderer section")
@@ -388,6 +390,8 @@ def run_ours(args):
         t0 = time.perf_counter()
         tuned = batch.autotune([r], [n], sample_fraction=1.0 / 8)
         tune_s = time.perf_counter() - t0
+    if args.frame_layout:
+        batch.configure(layout=args.frame_layout)
     stream = torch.cuda.current_stream(dev)
     film = torch.zeros(W * H * 3, dtype=torch.float32, device=dev)
 
