@@ -326,10 +326,10 @@ def _batch_launches(cfg, stats, bounces):
 def frame_roofline(prof_count, prof_time, layout="bvh"):
     """Roofline of the dominant kernel of the frame, the closest-hit
     traversal of the path queues (and, beside it, the shadow traversal):
-    algorithmic bytes (SURVEY d: 32 B ray + 16 B hit + 32 B per binary-node
-    slab test, 24 B for a quantised node, + 48 B per TriAccel test, counted
-    on the same samples by the counting kernel) over the launches' summed
-    device time."""
+    algorithmic bytes per ray (32 B ray + 16 B hit + 32 B per binary-node
+    slab test, 24 B for a quantised node, + 48 B per TriAccel test, the
+    tests counted on the same samples by the counting kernel) over the
+    launches' summed device time."""
     peak, peak_kind = measured_peaks()
     out = {}
     for kind in ("closest", "shadow"):
