@@ -138,7 +138,8 @@ typedef struct {
     int64_t num_leaves;
     int32_t max_depth;
     int32_t layout;
-    int64_t device_bytes;       /* acceleration + geometry bytes in HBM */
+    int64_t device_bytes;       /* bytes in HBM of the traversal data: every tree in both layouts,
+                                   the quantised render nodes and the triangle records */
     double build_seconds;       /* host BVH build time */
     float bounds_min[3];        /* Scene::GetAABBTriangles */
     float bounds_max[3];

@@ -457,13 +457,17 @@ int create_impl(const LmgpuSceneDesc* desc, LmgpuScene** out)
     info.max_depth = b.max_depth;
     info.layout = desc->layout;
     info.build_seconds = b.build_seconds;
+    // Everything uploaded for traversal: both layouts of each tree (a batch
+    // may pick either), the quantised copy of the render view's binary tree,
+    // and the triangle records.
     int64_t bytes = 0;
     bytes += (int64_t)b.tris.size() * sizeof(TriRecord);
-    bytes += (desc->layout == LMGPU_LAYOUT_BVH4 ? (int64_t)b.bvh4.size() * sizeof(Bvh4Node) : (int64_t)b.bvh2.size() * sizeof(Bvh2Node));
+    bytes += (int64_t)b.bvh4.size() * sizeof(Bvh4Node) + (int64_t)b.bvh2.size() * sizeof(Bvh2Node);
     if (render_tree) {
         bytes += (int64_t)b.rtris.size() * sizeof(TriRecord);
-        bytes += (desc->layout == LMGPU_LAYOUT_BVH4 ? (int64_t)b.rbvh4.size() * sizeof(Bvh4Node) : (int64_t)b.rbvh2.size() * sizeof(Bvh2Node));
+        bytes += (int64_t)b.rbvh4.size() * sizeof(Bvh4Node) + (int64_t)b.rbvh2.size() * sizeof(Bvh2Node);
     }
+    if (s->rdev.bvh2q) bytes += (int64_t)(render_tree ? b.rbvh2 : b.bvh2).size() * sizeof(Bvh2QNode);
     info.device_bytes = bytes;
     for (int c = 0; c < 3; c++) { info.bounds_min[c] = b.bounds.mn[c]; info.bounds_max[c] = b.bounds.mx[c]; }
     info.render_tree = render_tree ? LMGPU_RENDER_TREE_SAH : LMGPU_RENDER_TREE_REFERENCE;
