@@ -105,6 +105,7 @@ def test_batch_matches_one_scene_renders(cuda, technique):
     dict(mode="waves", layout="bvh_q16", wave_paths=10000, use_graph=False),
     dict(layout="bvh_qshadow"),                  # float nodes for bounce rays, quantised for shadow rays
     dict(mode="overlap", layout="bvh_qshadow", wave_paths=4096),
+    dict(mode="stream", layout="bvh_qshadow", wave_paths=4096),
 ])
 def test_batch_configurations_agree(cuda, config):
     items = small_set()
