@@ -73,12 +73,14 @@ def assert_same(got, want):
         np.testing.assert_allclose(g, w, rtol=1e-9, atol=1e-12)
 
 
+@pytest.mark.parametrize("layout", ["bvh", "bvh_qshadow"])
 @pytest.mark.parametrize("technique", ["pt.mis", "pt.direct", "pt"])
-def test_batch_matches_one_scene_renders(cuda, technique):
+def test_batch_matches_one_scene_renders(cuda, technique, layout):
     items = small_set(technique)
     built = [build(p) for p, _, _ in items]
     want = plain_films(built, items)
     batch = SceneBatch(built)
+    batch.configure(layout=layout)
     assert_same(batch_films(batch, items), want)
     st = batch.last_stats
     assert st["paths"] == sum(n for _, _, n in items)
